@@ -1,0 +1,126 @@
+/*
+ * mhd_gpu.h -- C ABI of the B200 (sm_100a) implementation of the per-step
+ * hot path of the 2-D compressible MHD solver MHD2DCFDFFTW.
+ *
+ * Two layers, both plain C (no C++ or torch types cross this boundary):
+ *
+ *  1. Handle-based API (mhdgpu_*): a context owns one 2-D periodic domain on
+ *     one GPU -- the state uu[NVAR][nx][ny], dudtRK and the derivative arrays
+ *     that the reference keeps as globals (initialize.h:11-69) -- and exposes
+ *     the reference's operators on it, whole RK3 stages and steps.
+ *  2. Drop-in layer: the reference's own entry points (derivX, derivY,
+ *     calcRHS, filtering, rkExecute, calcDt, ...) with the reference's
+ *     signatures, implemented over the reference's globals in
+ *     mhd2dcfdfftw_open_b200/csrc/dropin.c.  Declared in mhd_gpu_dropin.h.
+ *
+ * Layout: every field array is C order [nfield][nx][ny] of doubles
+ * (macros.h:4-24), y contiguous.  Variable order: rho, ux, uy, uz, Bx, By,
+ * Bz, p (and psi with hyperbolic cleaning).
+ *
+ * Errors: every call returns an mhdgpu_status; nothing traps or exits.
+ * mhdgpu_last_error() repeats the last non-OK status of the calling thread.
+ */
+#ifndef MHD_GPU_H
+#define MHD_GPU_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* The 15 lines of the reference's `input` file, in their order
+ * (input:1-15, parsed by readInput at initialize.c:456-525). */
+typedef struct {
+    int boundaryTypeX;   /* 0 periodic (supported), 1 open (rejected)      */
+    double cfl;
+    double Tmax;
+    double dtOut;
+    long nx;
+    long ny;             /* even, power of two, 8..8192                    */
+    double Lx;
+    double Ly;
+    double adiabaticIdx;
+    int Hall;            /* enters the CFL speed and forces d2B (no E term) */
+    double di;
+    double resistivity;
+    double viscosity;
+    int divBcleaning;    /* 0 none, 1 diffusive, 2 hyperbolic (NVAR = 9)   */
+    int outDivB;
+} mhdgpu_params;
+
+typedef enum {
+    MHDGPU_OK = 0,
+    MHDGPU_ERR_INVALID = 1,      /* bad argument or size                   */
+    MHDGPU_ERR_UNSUPPORTED = 2,  /* configuration outside the GPU path     */
+    MHDGPU_ERR_CUDA = 3,         /* a CUDA runtime call failed             */
+    MHDGPU_ERR_NOMEM = 4,        /* device allocation failed               */
+    MHDGPU_ERR_TIMEOUT = 5,      /* a bounded on-device wait ran out       */
+    MHDGPU_ERR_NONFINITE = 6     /* the state holds NaN/Inf or rho,p <= 0  */
+} mhdgpu_status;
+
+/* Arrays of a context, named after the reference's globals
+ * (initialize.h:19-27).  Field counts: NVAR for UU/DUDX/DUDY/DUDT/DUDTRK,
+ * 3 for the second derivatives and the electric field, 1 for divB. */
+typedef enum {
+    MHDGPU_UU = 0, MHDGPU_DUDX, MHDGPU_DUDY, MHDGPU_D2UDX2, MHDGPU_D2UDY2,
+    MHDGPU_D2BDX2, MHDGPU_D2BDY2, MHDGPU_DIVB, MHDGPU_DDIVBDX, MHDGPU_DDIVBDY,
+    MHDGPU_EFIELD, MHDGPU_DEDX, MHDGPU_DEDY, MHDGPU_DUDT, MHDGPU_DUDTRK,
+    MHDGPU_NARRAYS
+} mhdgpu_array;
+
+typedef struct mhdgpu_ctx mhdgpu_ctx;
+
+/* --- lifetime (replaces initialize()/finalize(), initialize.c:87-419) --- */
+int mhdgpu_read_input(const char *path, mhdgpu_params *out);
+int mhdgpu_create(const mhdgpu_params *p, int device, mhdgpu_ctx **out);
+void mhdgpu_destroy(mhdgpu_ctx *ctx);
+int mhdgpu_last_error(void);
+const char *mhdgpu_error_string(int status);
+int mhdgpu_nvar(const mhdgpu_ctx *ctx);
+
+/* --- host <-> device --------------------------------------------------- */
+int mhdgpu_set_array(mhdgpu_ctx *ctx, int which, const double *host);
+int mhdgpu_get_array(mhdgpu_ctx *ctx, int which, double *host);
+/* device address of a context array (for callers that keep data resident) */
+double *mhdgpu_device_array(mhdgpu_ctx *ctx, int which);
+int mhdgpu_synchronize(mhdgpu_ctx *ctx);
+
+/* --- operators on the context's arrays, mirroring the reference --------
+ * Each replaces the reference routine cited; all run asynchronously on the
+ * context's stream.                                                        */
+/* derivX / derivXX (calcDerivs.c:9-72): out[v] = d/dx (d2/dx2) of
+ * in[v + start], v < nv.  `in`/`out` are context arrays (mhdgpu_array). */
+int mhdgpu_deriv_x(mhdgpu_ctx *ctx, int nv, int in, int start, int out, int order);
+/* derivY / derivYY (calcDerivs.c:75-150) */
+int mhdgpu_deriv_y(mhdgpu_ctx *ctx, int nv, int in, int start, int out, int order);
+int mhdgpu_calc_efield(mhdgpu_ctx *ctx);   /* calcEfield, calcRHS.c:24-43 */
+int mhdgpu_calc_divb(mhdgpu_ctx *ctx);     /* calcDivB, calcRHS.c:13-22 */
+int mhdgpu_calc_rhs(mhdgpu_ctx *ctx);      /* calcRHS, calcRHS.c:46-75,498-544 */
+int mhdgpu_rk_init(mhdgpu_ctx *ctx, double dt);      /* rkInit, timeAdvance.c:20-27 */
+int mhdgpu_rk_execute(mhdgpu_ctx *ctx, int iRK);     /* rkExecute, timeAdvance.c:29-36 */
+int mhdgpu_filtering(mhdgpu_ctx *ctx);     /* filtering, filtering.c:98-102 */
+/* calcDt (timeAdvance.c:38-153); also sets Ch/Cp for hyperbolic cleaning */
+int mhdgpu_calc_dt(mhdgpu_ctx *ctx, double dt0, double *dt_out);
+/* checkDivB (mhd.c:342-367): max |dudx[Bx] + dudy[By]|, fills DIVB */
+int mhdgpu_check_divb(mhdgpu_ctx *ctx, double *maxdivb);
+int mhdgpu_get_cleaning_speeds(mhdgpu_ctx *ctx, double *Ch, double *Cp);
+
+/* --- whole stages and steps ------------------------------------------- */
+/* One RK3 stage, the body of mhd.c:154-199, through the operators above. */
+int mhdgpu_stage(mhdgpu_ctx *ctx, int iRK);
+/* nsteps RK3 steps.  dt_fixed > 0: fixed dt (calcDt still sets Ch/Cp with
+ * hyperbolic cleaning); dt_fixed <= 0: the reference's CFL control
+ * (mhd.c:58-63, 201-206).  *dt_io carries dt in and out. */
+int mhdgpu_steps(mhdgpu_ctx *ctx, int nsteps, double dt_fixed, double *dt_io);
+/* Same steps through the fused two-pass stage (x pass + y pass per stage). */
+int mhdgpu_steps_fused(mhdgpu_ctx *ctx, int nsteps, double dt_fixed, double *dt_io);
+
+/* --- diagnostics -------------------------------------------------------- */
+/* total energy, cross helicity (sums times dx*dy) and max|divB| of the last
+ * computed derivatives; *finite = 0 if the state holds NaN/Inf or rho,p<=0 */
+int mhdgpu_diagnostics(mhdgpu_ctx *ctx, double *energy, double *cross_helicity,
+                       int *finite);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,77 @@
+"""Build the sm_100a shared library in-tree.
+
+``python -m mhd2dcfdfftw_open_b200.build`` compiles every ``csrc/*.cu`` with
+nvcc for sm_100a (``-gencode arch=compute_100a,code=sm_100a``) into
+``mhd2dcfdfftw_open_b200/libmhdgpu.so`` and the drop-in object
+``csrc/dropin.c`` into ``libmhdgpu_dropin.a``.  No GPU is needed to build.
+"""
+from __future__ import annotations
+
+import glob
+import os
+import shutil
+import subprocess
+import sys
+
+PKG = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(PKG)
+CSRC = os.path.join(PKG, "csrc")
+LIB = os.path.join(PKG, "libmhdgpu.so")
+DROPIN = os.path.join(PKG, "libmhdgpu_dropin.a")
+BUILD_DIR = os.path.join(ROOT, "_build")
+
+NVCC_FLAGS = [
+    "-gencode", "arch=compute_100a,code=sm_100a",
+    "-O3", "-lineinfo", "-std=c++17",
+    "-Xcompiler", "-fPIC", "-Xcompiler", "-O3",
+    "--expt-relaxed-constexpr",
+]
+
+
+def nvcc() -> str:
+    for cand in (shutil.which("nvcc"), "/usr/local/cuda/bin/nvcc"):
+        if cand and os.path.exists(cand):
+            return cand
+    raise RuntimeError("nvcc not found")
+
+
+def _stale(target, sources):
+    if not os.path.exists(target):
+        return True
+    t = os.path.getmtime(target)
+    return any(os.path.getmtime(s) > t for s in sources)
+
+
+def build(force: bool = False, verbose: bool = False) -> str:
+    os.makedirs(BUILD_DIR, exist_ok=True)
+    cus = sorted(glob.glob(os.path.join(CSRC, "*.cu")))
+    hdrs = sorted(glob.glob(os.path.join(CSRC, "*.cuh")) +
+                  glob.glob(os.path.join(ROOT, "include", "*.h")))
+    objs = []
+    for cu in cus:
+        obj = os.path.join(BUILD_DIR, os.path.basename(cu) + ".o")
+        objs.append(obj)
+        if force or _stale(obj, [cu] + hdrs):
+            cmd = [nvcc()] + NVCC_FLAGS + ["-dc", cu, "-o", obj]
+            if verbose:
+                print(" ".join(cmd))
+            subprocess.run(cmd, check=True)
+    if force or _stale(LIB, objs):
+        cmd = [nvcc(), "-gencode", "arch=compute_100a,code=sm_100a", "-shared",
+               "-Xcompiler", "-fPIC", "-o", LIB] + objs + ["-lcudart"]
+        if verbose:
+            print(" ".join(cmd))
+        subprocess.run(cmd, check=True)
+    dropin_c = os.path.join(CSRC, "dropin.c")
+    if os.path.exists(dropin_c) and (force or _stale(DROPIN, [dropin_c] + hdrs)):
+        obj = os.path.join(BUILD_DIR, "dropin.o")
+        subprocess.run(["gcc", "-O2", "-fPIC", "-std=c99", "-c", dropin_c,
+                        "-I", os.path.join(ROOT, "include"), "-o", obj], check=True)
+        if os.path.exists(DROPIN):
+            os.remove(DROPIN)
+        subprocess.run(["ar", "rcs", DROPIN, obj], check=True)
+    return LIB
+
+
+if __name__ == "__main__":
+    build(force="--force" in sys.argv, verbose=True)

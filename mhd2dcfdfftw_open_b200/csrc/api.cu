@@ -1,0 +1,414 @@
+// C ABI of the sm_100a hot path (include/mhd_gpu.h): context lifetime, the
+// reference's operators on the context's arrays, and whole RK3 stages/steps.
+#include <cuda_runtime.h>
+
+#include <cctype>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <new>
+
+#include "common.cuh"
+
+using mhd::Ctx;
+
+static thread_local int g_last_error = MHDGPU_OK;
+
+int mhd_set_error(int status)
+{
+    g_last_error = status;
+    return status;
+}
+
+extern "C" int mhdgpu_last_error(void) { return g_last_error; }
+
+extern "C" const char *mhdgpu_error_string(int s)
+{
+    switch (s) {
+    case MHDGPU_OK: return "ok";
+    case MHDGPU_ERR_INVALID: return "invalid argument";
+    case MHDGPU_ERR_UNSUPPORTED: return "configuration not supported by the GPU path";
+    case MHDGPU_ERR_CUDA: return "CUDA runtime error";
+    case MHDGPU_ERR_NOMEM: return "device memory exhausted";
+    case MHDGPU_ERR_TIMEOUT: return "bounded device wait ran out";
+    case MHDGPU_ERR_NONFINITE: return "state is not finite or not positive";
+    default: return "unknown status";
+    }
+}
+
+// readInput (initialize.c:442-525): 15 lines, the first 16 characters of
+// each converted with atoi/atof.
+extern "C" int mhdgpu_read_input(const char *path, mhdgpu_params *o)
+{
+    if (!path || !o) return mhd_set_error(MHDGPU_ERR_INVALID);
+    FILE *fp = fopen(path, "r");
+    if (!fp) return mhd_set_error(MHDGPU_ERR_INVALID);
+    char line[256], v[17];
+    double d[15];
+    for (int k = 0; k < 15; k++) {
+        if (!fgets(line, sizeof line, fp)) {
+            fclose(fp);
+            return mhd_set_error(MHDGPU_ERR_INVALID);
+        }
+        memcpy(v, line, 16);
+        v[16] = 0;
+        d[k] = (k == 0 || k == 4 || k == 5 || k == 9 || k == 13 || k == 14) ? (double)atoi(v) : atof(v);
+    }
+    fclose(fp);
+    o->boundaryTypeX = (int)d[0];
+    o->cfl = d[1];
+    o->Tmax = d[2];
+    o->dtOut = d[3];
+    o->nx = (long)d[4];
+    o->ny = (long)d[5];
+    o->Lx = d[6];
+    o->Ly = d[7];
+    o->adiabaticIdx = d[8];
+    o->Hall = (int)d[9];
+    o->di = d[10];
+    o->resistivity = d[11];
+    o->viscosity = d[12];
+    o->divBcleaning = (int)d[13];
+    o->outDivB = (int)d[14];
+    return MHDGPU_OK;
+}
+
+static int fields_of(const Ctx *c, int which)
+{
+    const mhdgpu_params &p = c->p;
+    switch (which) {
+    case MHDGPU_UU: case MHDGPU_DUDX: case MHDGPU_DUDY: case MHDGPU_DUDT: case MHDGPU_DUDTRK:
+        return c->nvar;
+    case MHDGPU_D2UDX2: case MHDGPU_D2UDY2:
+        return p.viscosity > 0 ? 3 : 0;
+    case MHDGPU_D2BDX2: case MHDGPU_D2BDY2:
+        return (p.resistivity > 0 || p.Hall == 1) ? 3 : 0;
+    case MHDGPU_DIVB:
+        return 1;
+    case MHDGPU_DDIVBDX: case MHDGPU_DDIVBDY:
+        return p.divBcleaning == 1 ? 1 : 0;
+    case MHDGPU_EFIELD: case MHDGPU_DEDX: case MHDGPU_DEDY:
+        return 3;
+    default:
+        return -1;
+    }
+}
+
+extern "C" void mhdgpu_destroy(mhdgpu_ctx *h)
+{
+    Ctx *c = reinterpret_cast<Ctx *>(h);
+    if (!c) return;
+    cudaSetDevice(c->device);
+    if (c->stream) cudaStreamSynchronize(c->stream);
+    mhd::fused_free(c);
+    mhd::xsolve_free(c);
+    mhd::yspec_free(c);
+    for (int k = 0; k < MHDGPU_NARRAYS; k++) cudaFree(c->arr[k]);
+    cudaFree(c->dscal);
+    cudaFree(c->dred);
+    cudaFree(c->dflag);
+    if (c->stream) cudaStreamDestroy(c->stream);
+    delete c;
+}
+
+static bool valid_params(const mhdgpu_params *p)
+{
+    if (!p) return false;
+    if (p->nx < 8 || p->ny < 8 || p->ny > 8192 || (p->ny & (p->ny - 1)) != 0) return false;
+    if (!(p->Lx > 0) || !(p->Ly > 0) || !(p->adiabaticIdx > 1)) return false;
+    if (p->divBcleaning < 0 || p->divBcleaning > 2) return false;
+    return true;
+}
+
+extern "C" int mhdgpu_create(const mhdgpu_params *p, int device, mhdgpu_ctx **out)
+{
+    if (!out) return mhd_set_error(MHDGPU_ERR_INVALID);
+    *out = nullptr;
+    if (!valid_params(p)) return mhd_set_error(MHDGPU_ERR_INVALID);
+    // The open x boundary (boundaryTypeX = 1) is not on the GPU path; the
+    // reference's own single-rank open boundary is inconsistent
+    // (parallel.c:34-61 fills only one halo side).
+    if (p->boundaryTypeX != 0) return mhd_set_error(MHDGPU_ERR_UNSUPPORTED);
+    Ctx *c = new (std::nothrow) Ctx();
+    if (!c) return mhd_set_error(MHDGPU_ERR_NOMEM);
+    memset(c, 0, sizeof *c);
+    c->p = *p;
+    c->device = device;
+    c->nvar = p->divBcleaning == 2 ? 9 : 8;  // initialize.c:207-214
+    c->nx = p->nx;
+    c->ny = p->ny;
+    c->dx = p->Lx / (double)p->nx;            // initialize.c:125-135
+    c->dy = p->Ly / (double)p->ny;
+    double mx = c->dx > c->dy ? c->dx : c->dy;
+    c->const_diff_divb = 2.0 * mx * mx;       // initialize.c:17, 154
+    c->Ch = c->Cp = 0.0;
+    int rc = MHDGPU_OK;
+    auto fail = [&](int s) {
+        mhdgpu_destroy(reinterpret_cast<mhdgpu_ctx *>(c));
+        return mhd_set_error(s);
+    };
+    if (cudaSetDevice(device) != cudaSuccess) return fail(MHDGPU_ERR_CUDA);
+    if (cudaDeviceGetAttribute(&c->sm_count, cudaDevAttrMultiProcessorCount, device) != cudaSuccess)
+        return fail(MHDGPU_ERR_CUDA);
+    if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess)
+        return fail(MHDGPU_ERR_CUDA);
+    const size_t plane = (size_t)c->nx * c->ny;
+    for (int k = 0; k < MHDGPU_NARRAYS; k++) {
+        int nf = fields_of(c, k);
+        c->arr_fields[k] = nf;
+        if (nf > 0) {
+            if (cudaMalloc(&c->arr[k], sizeof(double) * plane * nf) != cudaSuccess)
+                return fail(MHDGPU_ERR_NOMEM);
+            if (cudaMemset(c->arr[k], 0, sizeof(double) * plane * nf) != cudaSuccess)
+                return fail(MHDGPU_ERR_CUDA);
+        }
+    }
+    c->nred = 8192;
+    if (cudaMalloc(&c->dscal, sizeof(double) * 16) != cudaSuccess) return fail(MHDGPU_ERR_NOMEM);
+    if (cudaMalloc(&c->dred, sizeof(double) * c->nred) != cudaSuccess) return fail(MHDGPU_ERR_NOMEM);
+    if (cudaMalloc(&c->dflag, sizeof(int) * 4) != cudaSuccess) return fail(MHDGPU_ERR_NOMEM);
+    cudaMemset(c->dscal, 0, sizeof(double) * 16);
+    cudaMemset(c->dflag, 0, sizeof(int) * 4);
+    if ((rc = mhd::xsolve_setup(c)) != MHDGPU_OK) return fail(rc);
+    if ((rc = mhd::yspec_setup(c)) != MHDGPU_OK) return fail(rc);
+    if ((rc = mhd::fused_setup(c)) != MHDGPU_OK) return fail(rc);
+    if (cudaDeviceSynchronize() != cudaSuccess) return fail(MHDGPU_ERR_CUDA);
+    *out = reinterpret_cast<mhdgpu_ctx *>(c);
+    return MHDGPU_OK;
+}
+
+extern "C" int mhdgpu_nvar(const mhdgpu_ctx *h)
+{
+    return h ? reinterpret_cast<const Ctx *>(h)->nvar : -1;
+}
+
+#define CTX_OR_FAIL(h)                                          \
+    Ctx *c = reinterpret_cast<Ctx *>(h);                        \
+    if (!c) return mhd_set_error(MHDGPU_ERR_INVALID);           \
+    if (cudaSetDevice(c->device) != cudaSuccess) return mhd_set_error(MHDGPU_ERR_CUDA)
+
+extern "C" double *mhdgpu_device_array(mhdgpu_ctx *h, int which)
+{
+    Ctx *c = reinterpret_cast<Ctx *>(h);
+    if (!c || which < 0 || which >= MHDGPU_NARRAYS) return nullptr;
+    return c->arr[which];
+}
+
+extern "C" int mhdgpu_set_array(mhdgpu_ctx *h, int which, const double *host)
+{
+    CTX_OR_FAIL(h);
+    if (which < 0 || which >= MHDGPU_NARRAYS || !host || !c->arr[which])
+        return mhd_set_error(MHDGPU_ERR_INVALID);
+    size_t n = (size_t)c->arr_fields[which] * c->nx * c->ny;
+    MHD_CUDA_TRY(cudaMemcpyAsync(c->arr[which], host, n * sizeof(double), cudaMemcpyHostToDevice,
+                                 c->stream));
+    MHD_CUDA_TRY(cudaStreamSynchronize(c->stream));
+    if (which == MHDGPU_UU) c->fused_pending_filter = 0;
+    return MHDGPU_OK;
+}
+
+extern "C" int mhdgpu_get_array(mhdgpu_ctx *h, int which, double *host)
+{
+    CTX_OR_FAIL(h);
+    if (which < 0 || which >= MHDGPU_NARRAYS || !host || !c->arr[which])
+        return mhd_set_error(MHDGPU_ERR_INVALID);
+    size_t n = (size_t)c->arr_fields[which] * c->nx * c->ny;
+    MHD_CUDA_TRY(cudaMemcpyAsync(host, c->arr[which], n * sizeof(double), cudaMemcpyDeviceToHost,
+                                 c->stream));
+    MHD_CUDA_TRY(cudaStreamSynchronize(c->stream));
+    return MHDGPU_OK;
+}
+
+static int check_flag(Ctx *c)
+{
+    int f = 0;
+    MHD_CUDA_TRY(cudaMemcpyAsync(&f, c->dflag, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+    MHD_CUDA_TRY(cudaStreamSynchronize(c->stream));
+    if (f != 0) {
+        cudaMemsetAsync(c->dflag, 0, sizeof(int), c->stream);
+        return mhd_set_error(f);
+    }
+    return MHDGPU_OK;
+}
+
+extern "C" int mhdgpu_synchronize(mhdgpu_ctx *h)
+{
+    CTX_OR_FAIL(h);
+    MHD_CUDA_TRY(cudaStreamSynchronize(c->stream));
+    return check_flag(c);
+}
+
+// ---------------------------------------------------------------------------
+// operators
+// ---------------------------------------------------------------------------
+static bool arr_ok(const Ctx *c, int which, int first, int nv)
+{
+    return which >= 0 && which < MHDGPU_NARRAYS && c->arr[which] && first >= 0 &&
+           first + nv <= c->arr_fields[which];
+}
+
+extern "C" int mhdgpu_deriv_x(mhdgpu_ctx *h, int nv, int in, int start, int out, int order)
+{
+    CTX_OR_FAIL(h);
+    if (order != 1 && order != 2) return mhd_set_error(MHDGPU_ERR_INVALID);
+    if (!arr_ok(c, in, start, nv) || !arr_ok(c, out, 0, nv)) return mhd_set_error(MHDGPU_ERR_INVALID);
+    return mhd::launch_xsolve(c, order == 1 ? mhd::XOP_D1 : mhd::XOP_D2, nv, c->arr[in], start,
+                              c->arr[out], 0);
+}
+
+extern "C" int mhdgpu_deriv_y(mhdgpu_ctx *h, int nv, int in, int start, int out, int order)
+{
+    CTX_OR_FAIL(h);
+    if (order != 1 && order != 2) return mhd_set_error(MHDGPU_ERR_INVALID);
+    if (!arr_ok(c, in, start, nv) || !arr_ok(c, out, 0, nv)) return mhd_set_error(MHDGPU_ERR_INVALID);
+    return mhd::launch_yspec(c, order - 1, nv, c->arr[in], start, c->arr[out], 0);
+}
+
+extern "C" int mhdgpu_calc_efield(mhdgpu_ctx *h)
+{
+    CTX_OR_FAIL(h);
+    return mhd::launch_efield(c);
+}
+
+extern "C" int mhdgpu_calc_divb(mhdgpu_ctx *h)
+{
+    CTX_OR_FAIL(h);
+    return mhd::launch_divb(c, c->arr[MHDGPU_DIVB]);
+}
+
+extern "C" int mhdgpu_calc_rhs(mhdgpu_ctx *h)
+{
+    CTX_OR_FAIL(h);
+    return mhd::launch_rhs(c);
+}
+
+// rkInit (timeAdvance.c:20-27): stage coefficients and dudtRK = 0
+extern "C" int mhdgpu_rk_init(mhdgpu_ctx *h, double dt)
+{
+    CTX_OR_FAIL(h);
+    c->dt = dt;
+    c->cc[0] = 8.0 / 15.0 * dt;
+    c->dd[0] = 0.0;
+    c->cc[1] = 5.0 / 12.0 * dt;
+    c->dd[1] = -17. / 60. * dt;
+    c->cc[2] = 0.75 * dt;
+    c->dd[2] = -5. / 12. * dt;
+    MHD_CUDA_TRY(cudaMemsetAsync(c->arr[MHDGPU_DUDTRK], 0,
+                                 sizeof(double) * c->nvar * c->nx * c->ny, c->stream));
+    return MHDGPU_OK;
+}
+
+extern "C" int mhdgpu_rk_execute(mhdgpu_ctx *h, int iRK)
+{
+    CTX_OR_FAIL(h);
+    if (iRK < 0 || iRK > 2) return mhd_set_error(MHDGPU_ERR_INVALID);
+    return mhd::launch_rk(c, iRK);
+}
+
+// filtering (filtering.c:98-102): x filter of all NVAR fields, then y filter,
+// both in place on uu
+extern "C" int mhdgpu_filtering(mhdgpu_ctx *h)
+{
+    CTX_OR_FAIL(h);
+    int rc = mhd::launch_xsolve(c, mhd::XOP_F, c->nvar, c->arr[MHDGPU_UU], 0, c->arr[MHDGPU_UU], 0);
+    if (rc) return rc;
+    return mhd::launch_yspec(c, 2, c->nvar, c->arr[MHDGPU_UU], 0, c->arr[MHDGPU_UU], 0);
+}
+
+extern "C" int mhdgpu_calc_dt(mhdgpu_ctx *h, double dt0, double *dt_out)
+{
+    CTX_OR_FAIL(h);
+    return mhd::launch_calc_dt(c, dt0, dt_out);
+}
+
+extern "C" int mhdgpu_check_divb(mhdgpu_ctx *h, double *maxdivb)
+{
+    CTX_OR_FAIL(h);
+    if (!maxdivb) return mhd_set_error(MHDGPU_ERR_INVALID);
+    return mhd::launch_max_divb(c, maxdivb);
+}
+
+extern "C" int mhdgpu_get_cleaning_speeds(mhdgpu_ctx *h, double *Ch, double *Cp)
+{
+    CTX_OR_FAIL(h);
+    if (Ch) *Ch = c->Ch;
+    if (Cp) *Cp = c->Cp;
+    return MHDGPU_OK;
+}
+
+// ---------------------------------------------------------------------------
+// stages and steps
+// ---------------------------------------------------------------------------
+#define TRY(x)                  \
+    do {                        \
+        int r_ = (x);           \
+        if (r_) return r_;      \
+    } while (0)
+
+// One RK3 stage with the reference's call order (mhd.c:154-199); the halo
+// exchanges are index wrap-around inside the x kernels.
+extern "C" int mhdgpu_stage(mhdgpu_ctx *h, int iRK)
+{
+    CTX_OR_FAIL(h);
+    if (iRK < 0 || iRK > 2) return mhd_set_error(MHDGPU_ERR_INVALID);
+    if (c->fused_pending_filter) return mhd_set_error(MHDGPU_ERR_INVALID);
+    const mhdgpu_params &p = c->p;
+    TRY(mhdgpu_deriv_x(h, c->nvar, MHDGPU_UU, 0, MHDGPU_DUDX, 1));
+    TRY(mhdgpu_deriv_y(h, c->nvar, MHDGPU_UU, 0, MHDGPU_DUDY, 1));
+    if (p.viscosity > 0) {
+        TRY(mhdgpu_deriv_x(h, 3, MHDGPU_UU, 1, MHDGPU_D2UDX2, 2));
+        TRY(mhdgpu_deriv_y(h, 3, MHDGPU_UU, 1, MHDGPU_D2UDY2, 2));
+    }
+    if (p.Hall == 1 || p.resistivity > 0) {
+        TRY(mhdgpu_deriv_x(h, 3, MHDGPU_UU, 4, MHDGPU_D2BDX2, 2));
+        TRY(mhdgpu_deriv_y(h, 3, MHDGPU_UU, 4, MHDGPU_D2BDY2, 2));
+    }
+    if (p.divBcleaning == 1) {
+        TRY(mhdgpu_calc_divb(h));
+        TRY(mhdgpu_deriv_x(h, 1, MHDGPU_DIVB, 0, MHDGPU_DDIVBDX, 1));
+        TRY(mhdgpu_deriv_y(h, 1, MHDGPU_DIVB, 0, MHDGPU_DDIVBDY, 1));
+    }
+    TRY(mhdgpu_calc_efield(h));
+    TRY(mhdgpu_deriv_x(h, 3, MHDGPU_EFIELD, 0, MHDGPU_DEDX, 1));
+    TRY(mhdgpu_deriv_y(h, 3, MHDGPU_EFIELD, 0, MHDGPU_DEDY, 1));
+    TRY(mhdgpu_calc_rhs(h));
+    TRY(mhdgpu_rk_execute(h, iRK));
+    TRY(mhdgpu_filtering(h));
+    return MHDGPU_OK;
+}
+
+// dt before the first step or after a step: fixed dt (with calcDt still run
+// for Ch/Cp under hyperbolic cleaning) or the reference's CFL control
+static int next_dt(mhdgpu_ctx *h, Ctx *c, double dt_fixed, double *dt)
+{
+    if (dt_fixed > 0) {
+        if (c->p.divBcleaning == 2) TRY(mhd::launch_calc_dt(c, dt_fixed, nullptr));
+        *dt = dt_fixed;
+        return MHDGPU_OK;
+    }
+    return mhd::launch_calc_dt(c, *dt, dt);
+}
+
+extern "C" int mhdgpu_steps(mhdgpu_ctx *h, int nsteps, double dt_fixed, double *dt_io)
+{
+    CTX_OR_FAIL(h);
+    if (nsteps < 0) return mhd_set_error(MHDGPU_ERR_INVALID);
+    double dt = dt_io ? *dt_io : 0.0;
+    TRY(next_dt(h, c, dt_fixed, &dt));
+    TRY(mhdgpu_rk_init(h, dt));
+    for (int s = 0; s < nsteps; s++) {
+        for (int k = 0; k < 3; k++) TRY(mhdgpu_stage(h, k));
+        TRY(next_dt(h, c, dt_fixed, &dt));
+        TRY(mhdgpu_rk_init(h, dt));
+    }
+    if (dt_io) *dt_io = dt;
+    MHD_CUDA_TRY(cudaStreamSynchronize(c->stream));
+    return check_flag(c);
+}
+
+extern "C" int mhdgpu_diagnostics(mhdgpu_ctx *h, double *energy, double *cross_helicity, int *finite)
+{
+    CTX_OR_FAIL(h);
+    return mhd::launch_diagnostics(c, energy, cross_helicity, finite);
+}

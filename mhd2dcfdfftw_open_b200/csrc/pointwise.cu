@@ -1,0 +1,428 @@
+// Pointwise operators and reductions of the hot path:
+//   calcEfield (calcRHS.c:24-43), calcDivB (calcRHS.c:13-22),
+//   calcRHSInnerPoint + addSourceTerm (calcRHS.c:77-161, 498-544),
+//   rkExecute (timeAdvance.c:29-36), calcDt (timeAdvance.c:38-153),
+//   checkDivB (mhd.c:342-367) and the energy / cross-helicity diagnostics.
+// All are HBM-streaming kernels over the [field][nx][ny] planes; the
+// reductions write one partial per block and finish in a second, single-block
+// pass in a fixed order, so their results do not depend on scheduling.
+#include <cmath>
+
+#include "common.cuh"
+
+namespace mhd {
+
+constexpr int PT = 256;
+
+static int grid_for(const Ctx *c, long n)
+{
+    long b = (n + PT - 1) / PT;
+    long cap = (long)c->sm_count * 8;
+    return (int)(b < cap ? b : cap);
+}
+
+__global__ void efield_kernel(const double *__restrict__ uu, double *__restrict__ E, long plane)
+{
+    for (long o = blockIdx.x * (long)blockDim.x + threadIdx.x; o < plane;
+         o += (long)gridDim.x * blockDim.x) {
+        double ux = uu[UX * plane + o], uy = uu[UY * plane + o], uz = uu[UZ * plane + o];
+        double bx = uu[BX * plane + o], by = uu[BY * plane + o], bz = uu[BZ * plane + o];
+        E[o] = uz * by - uy * bz;
+        E[plane + o] = ux * bz - uz * bx;
+        E[2 * plane + o] = uy * bx - ux * by;
+    }
+}
+
+__global__ void divb_kernel(const double *__restrict__ dudx, const double *__restrict__ dudy,
+                            double *__restrict__ out, long plane)
+{
+    for (long o = blockIdx.x * (long)blockDim.x + threadIdx.x; o < plane;
+         o += (long)gridDim.x * blockDim.x)
+        out[o] = dudx[BX * plane + o] + dudy[BY * plane + o];
+}
+
+struct RhsArgs {
+    const double *uu, *dudx, *dudy, *dEdx, *dEdy;
+    const double *d2udx2, *d2udy2, *d2Bdx2, *d2Bdy2, *ddivBdx, *ddivBdy;
+    double *dudt;
+    long plane;
+    double gamma, visc, resist, cdiff, Ch, Cp;
+    int cleaning;
+};
+
+// calcRHSInnerPoint on the whole periodic domain, then addSourceTerm; the
+// expressions keep the reference's order of operations.
+__global__ void rhs_kernel(RhsArgs a)
+{
+    const long plane = a.plane;
+    for (long o = blockIdx.x * (long)blockDim.x + threadIdx.x; o < plane;
+         o += (long)gridDim.x * blockDim.x) {
+        const double *u = a.uu, *dx = a.dudx, *dy = a.dudy;
+#define F(arr, v) arr[(v) * plane + o]
+        double rho = F(u, RHO), ux = F(u, UX), uy = F(u, UY);
+        double bx = F(u, BX), by = F(u, BY), bz = F(u, BZ), pr = F(u, P);
+        double divU = F(dx, UX) + F(dy, UY);
+        double divB = F(dx, BX) + F(dy, BY);
+        double jx = F(dy, BZ);
+        double jy = -F(dx, BZ);
+        double jz = F(dx, BY) - F(dy, BX);
+        double r_rho = -rho * divU - ux * F(dx, RHO) - uy * F(dy, RHO);
+        double r_ux = -ux * F(dx, UX) - uy * F(dy, UX) - F(dx, P) / rho + jy * bz / rho - jz * by / rho;
+        double r_uy = -ux * F(dx, UY) - uy * F(dy, UY) - F(dy, P) / rho + jz * bx / rho - jx * bz / rho;
+        double r_uz = -ux * F(dx, UZ) - uy * F(dy, UZ) + jx * by / rho - jy * bx / rho;
+        double r_bx = -a.dEdy[2 * plane + o];
+        double r_by = a.dEdx[2 * plane + o];
+        double r_bz = a.dEdy[o] - a.dEdx[plane + o];
+        double r_p = -ux * F(dx, P) - uy * F(dy, P) - a.gamma * pr * divU;
+        double r_psi = 0.0;
+        if (a.cleaning == 2) {
+            r_ux = r_ux - divB * bx;
+            r_uy = r_uy - divB * by;
+            r_uz = r_uz - divB * bz;
+            r_bx = r_bx - F(dx, PSI);
+            r_by = r_by - F(dy, PSI);
+            r_psi = -a.Ch * a.Ch * (divB + F(u, PSI) / a.Cp / a.Cp);
+        }
+        if (a.visc > 0) {
+            r_ux = r_ux + a.visc / rho * (a.d2udx2[o] + a.d2udy2[o]);
+            r_uy = r_uy + a.visc / rho * (a.d2udx2[plane + o] + a.d2udy2[plane + o]);
+            r_uz = r_uz + a.visc / rho * (a.d2udx2[2 * plane + o] + a.d2udy2[2 * plane + o]);
+        }
+        if (a.resist > 0) {
+            r_bx = r_bx + a.resist * (a.d2Bdx2[o] + a.d2Bdy2[o]);
+            r_by = r_by + a.resist * (a.d2Bdx2[plane + o] + a.d2Bdy2[plane + o]);
+            r_bz = r_bz + a.resist * (a.d2Bdx2[2 * plane + o] + a.d2Bdy2[2 * plane + o]);
+        }
+        if (a.cleaning == 1) {
+            r_bx = r_bx + a.cdiff * a.ddivBdx[o];
+            r_by = r_by + a.cdiff * a.ddivBdy[o];
+        }
+        double *d = a.dudt;
+        F(d, RHO) = r_rho; F(d, UX) = r_ux; F(d, UY) = r_uy; F(d, UZ) = r_uz;
+        F(d, BX) = r_bx; F(d, BY) = r_by; F(d, BZ) = r_bz; F(d, P) = r_p;
+        if (a.cleaning == 2) F(d, PSI) = r_psi;
+#undef F
+    }
+}
+
+__global__ void rk_kernel(double *__restrict__ uu, const double *__restrict__ dudt,
+                          double *__restrict__ dudtRK, long n, double cc, double dd)
+{
+    for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n;
+         i += (long)gridDim.x * blockDim.x) {
+        double d = dudt[i];
+        uu[i] = uu[i] + cc * d + dd * dudtRK[i];
+        dudtRK[i] = d;
+    }
+}
+
+// --- reductions ------------------------------------------------------------
+__device__ __forceinline__ double warp_min(double v)
+{
+    for (int o = 16; o > 0; o >>= 1) v = fmin(v, __shfl_xor_sync(0xffffffffu, v, o));
+    return v;
+}
+__device__ __forceinline__ double warp_max(double v)
+{
+    for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+    return v;
+}
+__device__ __forceinline__ double warp_sum(double v)
+{
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+struct DtArgs {
+    const double *uu;
+    long plane, ny;
+    double gamma, dx, dy, di, resist, visc;
+    int hall;
+    double *part;
+};
+
+// cmaxx, cmaxy of one cell (timeAdvance.c:55-105)
+__device__ __forceinline__ void cell_speeds(const DtArgs &a, long o, double &cmaxx, double &cmaxy)
+{
+    const long plane = a.plane;
+    const double *u = a.uu;
+    double rho = u[RHO * plane + o];
+    double csound2 = a.gamma * u[P * plane + o] / rho;
+    double sr = sqrt(rho);
+    double cax = u[BX * plane + o] / sr, cay = u[BY * plane + o] / sr, caz = u[BZ * plane + o] / sr;
+    double ca2 = cax * cax + cay * cay + caz * caz;
+    double cms2 = csound2 + ca2;
+    double cnsx2 = sqrt(fmax(cms2 * cms2 - 4 * csound2 * cax * cax, 0.));
+    double cnsy2 = sqrt(fmax(cms2 * cms2 - 4 * csound2 * cay * cay, 0.));
+    const double s2 = sqrt(2.);
+    double cfx = sqrt(cms2 + cnsx2) / s2, cfy = sqrt(cms2 + cnsy2) / s2;
+    double csx = sqrt(fmax(cms2 - cnsx2, 0.)) / s2, csy = sqrt(fmax(cms2 - cnsy2, 0.)) / s2;
+    double ux = u[UX * plane + o], uy = u[UY * plane + o];
+    double t = fmax(fabs(ux), fabs(ux - cax));
+    t = fmax(fabs(ux - csx), t);
+    t = fmax(fabs(ux - cfx), t);
+    t = fmax(fabs(ux + cax), t);
+    t = fmax(fabs(ux + csx), t);
+    cmaxx = fmax(fabs(ux + cfx), t);
+    t = fmax(fabs(uy), fabs(uy - cay));
+    t = fmax(fabs(uy - csy), t);
+    t = fmax(fabs(uy - cfy), t);
+    t = fmax(fabs(uy + cay), t);
+    t = fmax(fabs(uy + csy), t);
+    cmaxy = fmax(fabs(uy + cfy), t);
+    if (a.hall == 1) {
+        double ch = a.di / fmin(a.dx, a.dy) / rho *
+                    fmax(fabs(u[BX * plane + o]), fmax(fabs(u[BY * plane + o]), fabs(u[BZ * plane + o])));
+        cmaxx = fmax(cmaxx, ch);
+        cmaxy = fmax(cmaxy, ch);
+    }
+}
+
+__global__ void dt_partial_kernel(DtArgs a)
+{
+    double mn = INFINITY;
+    for (long o = blockIdx.x * (long)blockDim.x + threadIdx.x; o < a.plane;
+         o += (long)gridDim.x * blockDim.x) {
+        double cx, cy;
+        cell_speeds(a, o, cx, cy);
+        double dtx = a.dx / cx, dty = a.dy / cy;
+        if (a.resist > 0) {
+            dtx = fmin(dtx, a.dx * a.dx / a.resist);
+            dty = fmin(dty, a.dy * a.dy / a.resist);
+        }
+        if (a.visc > 0) {
+            dtx = fmin(dtx, a.dx * a.dx / a.visc);
+            dty = fmin(dty, a.dy * a.dy / a.visc);
+        }
+        mn = fmin(mn, fmin(dtx, dty));
+    }
+    __shared__ double sm[PT / 32];
+    mn = warp_min(mn);
+    if ((threadIdx.x & 31) == 0) sm[threadIdx.x >> 5] = mn;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        double v = threadIdx.x < blockDim.x / 32 ? sm[threadIdx.x] : INFINITY;
+        v = warp_min(v);
+        if (threadIdx.x == 0) a.part[blockIdx.x] = v;
+    }
+}
+
+// scal[0] = dt after the 2% hysteresis (timeAdvance.c:142-152); with
+// hyperbolic cleaning scal[1] = Ch = max(cmaxx, cmaxy) of the LAST cell of
+// the reference's loop (timeAdvance.c:107-112) and scal[2] = Cp = sqrt(Cr Ch)
+// (divBcleaning.c:4-10).
+__global__ void dt_final_kernel(DtArgs a, int nparts, double cfl, double dt0, int cleaning,
+                                double *scal)
+{
+    double mn = INFINITY;
+    for (int i = threadIdx.x; i < nparts; i += blockDim.x) mn = fmin(mn, a.part[i]);
+    __shared__ double sm[32];
+    mn = warp_min(mn);
+    if ((threadIdx.x & 31) == 0) sm[threadIdx.x >> 5] = mn;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double v = INFINITY;
+        for (int w = 0; w < (int)(blockDim.x / 32); w++) v = fmin(v, sm[w]);
+        double dtmin = v * cfl;
+        scal[0] = (dt0 < 0.98 * dtmin || dt0 > 1.02 * dtmin) ? dtmin : dt0;
+        if (cleaning == 2) {
+            double cx, cy;
+            cell_speeds(a, a.plane - 1, cx, cy);
+            double ch = fmax(cx, cy);
+            scal[1] = ch;
+            scal[2] = sqrt(0.18 * ch);
+        }
+    }
+}
+
+__global__ void maxdivb_kernel(const double *__restrict__ dudx, const double *__restrict__ dudy,
+                               double *__restrict__ divb, long plane, double *part)
+{
+    double mx = 0.0;
+    for (long o = blockIdx.x * (long)blockDim.x + threadIdx.x; o < plane;
+         o += (long)gridDim.x * blockDim.x) {
+        double v = dudx[BX * plane + o] + dudy[BY * plane + o];
+        divb[o] = v;
+        mx = fmax(mx, fabs(v));
+    }
+    __shared__ double sm[PT / 32];
+    mx = warp_max(mx);
+    if ((threadIdx.x & 31) == 0) sm[threadIdx.x >> 5] = mx;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        double v = threadIdx.x < blockDim.x / 32 ? sm[threadIdx.x] : 0.0;
+        v = warp_max(v);
+        if (threadIdx.x == 0) part[blockIdx.x] = v;
+    }
+}
+
+__global__ void diag_kernel(const double *__restrict__ uu, long plane, double gamma, double *part)
+{
+    double e = 0.0, h = 0.0, bad = 0.0;
+    for (long o = blockIdx.x * (long)blockDim.x + threadIdx.x; o < plane;
+         o += (long)gridDim.x * blockDim.x) {
+        double rho = uu[RHO * plane + o], ux = uu[UX * plane + o], uy = uu[UY * plane + o];
+        double uz = uu[UZ * plane + o], bx = uu[BX * plane + o], by = uu[BY * plane + o];
+        double bz = uu[BZ * plane + o], p = uu[P * plane + o];
+        e += 0.5 * rho * (ux * ux + uy * uy + uz * uz) + 0.5 * (bx * bx + by * by + bz * bz) +
+             p / (gamma - 1.0);
+        h += ux * bx + uy * by + uz * bz;
+        double s = rho + ux + uy + uz + bx + by + bz + p;
+        if (!isfinite(s) || !(rho > 0) || !(p > 0)) bad += 1.0;
+    }
+    __shared__ double sm[3][PT / 32];
+    e = warp_sum(e); h = warp_sum(h); bad = warp_sum(bad);
+    if ((threadIdx.x & 31) == 0) {
+        sm[0][threadIdx.x >> 5] = e; sm[1][threadIdx.x >> 5] = h; sm[2][threadIdx.x >> 5] = bad;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double s0 = 0, s1 = 0, s2 = 0;
+        for (int w = 0; w < (int)(blockDim.x / 32); w++) { s0 += sm[0][w]; s1 += sm[1][w]; s2 += sm[2][w]; }
+        part[3 * blockIdx.x] = s0; part[3 * blockIdx.x + 1] = s1; part[3 * blockIdx.x + 2] = s2;
+    }
+}
+
+__global__ void reduce_final_kernel(const double *part, int nparts, int stride, int mode,
+                                    double *out)
+{
+    // mode 0: max of part[i*stride]; mode 1: sums of each of `stride` columns
+    if (threadIdx.x != 0) return;
+    if (mode == 0) {
+        double v = 0.0;
+        for (int i = 0; i < nparts; i++) v = fmax(v, part[i * stride]);
+        out[0] = v;
+    } else {
+        for (int k = 0; k < stride; k++) {
+            double s = 0.0;
+            for (int i = 0; i < nparts; i++) s += part[i * stride + k];
+            out[k] = s;
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// host launchers
+// ---------------------------------------------------------------------------
+int launch_efield(Ctx *c)
+{
+    long plane = c->nx * c->ny;
+    efield_kernel<<<grid_for(c, plane), PT, 0, c->stream>>>(c->arr[MHDGPU_UU],
+                                                             c->arr[MHDGPU_EFIELD], plane);
+    MHD_CHECK_LAUNCH();
+    return MHDGPU_OK;
+}
+
+int launch_divb(Ctx *c, double *out)
+{
+    long plane = c->nx * c->ny;
+    divb_kernel<<<grid_for(c, plane), PT, 0, c->stream>>>(c->arr[MHDGPU_DUDX], c->arr[MHDGPU_DUDY],
+                                                           out, plane);
+    MHD_CHECK_LAUNCH();
+    return MHDGPU_OK;
+}
+
+int launch_rhs(Ctx *c)
+{
+    RhsArgs a;
+    a.uu = c->arr[MHDGPU_UU];
+    a.dudx = c->arr[MHDGPU_DUDX];
+    a.dudy = c->arr[MHDGPU_DUDY];
+    a.dEdx = c->arr[MHDGPU_DEDX];
+    a.dEdy = c->arr[MHDGPU_DEDY];
+    a.d2udx2 = c->arr[MHDGPU_D2UDX2];
+    a.d2udy2 = c->arr[MHDGPU_D2UDY2];
+    a.d2Bdx2 = c->arr[MHDGPU_D2BDX2];
+    a.d2Bdy2 = c->arr[MHDGPU_D2BDY2];
+    a.ddivBdx = c->arr[MHDGPU_DDIVBDX];
+    a.ddivBdy = c->arr[MHDGPU_DDIVBDY];
+    a.dudt = c->arr[MHDGPU_DUDT];
+    a.plane = c->nx * c->ny;
+    a.gamma = c->p.adiabaticIdx;
+    a.visc = c->p.viscosity;
+    a.resist = c->p.resistivity;
+    a.cdiff = c->const_diff_divb;
+    a.Ch = c->Ch;
+    a.Cp = c->Cp;
+    a.cleaning = c->p.divBcleaning;
+    rhs_kernel<<<grid_for(c, a.plane), PT, 0, c->stream>>>(a);
+    MHD_CHECK_LAUNCH();
+    return MHDGPU_OK;
+}
+
+int launch_rk(Ctx *c, int iRK)
+{
+    long n = (long)c->nvar * c->nx * c->ny;
+    rk_kernel<<<grid_for(c, n), PT, 0, c->stream>>>(c->arr[MHDGPU_UU], c->arr[MHDGPU_DUDT],
+                                                     c->arr[MHDGPU_DUDTRK], n, c->cc[iRK],
+                                                     c->dd[iRK]);
+    MHD_CHECK_LAUNCH();
+    return MHDGPU_OK;
+}
+
+int launch_calc_dt(Ctx *c, double dt0, double *dt_out)
+{
+    DtArgs a;
+    a.uu = c->arr[MHDGPU_UU];
+    a.plane = c->nx * c->ny;
+    a.ny = c->ny;
+    a.gamma = c->p.adiabaticIdx;
+    a.dx = c->dx;
+    a.dy = c->dy;
+    a.di = c->p.di;
+    a.resist = c->p.resistivity;
+    a.visc = c->p.viscosity;
+    a.hall = c->p.Hall;
+    a.part = c->dred;
+    int g = grid_for(c, a.plane);
+    if (g > c->nred) g = c->nred;
+    dt_partial_kernel<<<g, PT, 0, c->stream>>>(a);
+    MHD_CHECK_LAUNCH();
+    dt_final_kernel<<<1, 1024, 0, c->stream>>>(a, g, c->p.cfl, dt0, c->p.divBcleaning, c->dscal);
+    MHD_CHECK_LAUNCH();
+    double h[3];
+    MHD_CUDA_TRY(cudaMemcpyAsync(h, c->dscal, sizeof h, cudaMemcpyDeviceToHost, c->stream));
+    MHD_CUDA_TRY(cudaStreamSynchronize(c->stream));
+    if (c->p.divBcleaning == 2) {
+        c->Ch = h[1];
+        c->Cp = h[2];
+    }
+    if (dt_out) *dt_out = h[0];
+    return MHDGPU_OK;
+}
+
+int launch_max_divb(Ctx *c, double *out)
+{
+    long plane = c->nx * c->ny;
+    int g = grid_for(c, plane);
+    if (g > c->nred) g = c->nred;
+    maxdivb_kernel<<<g, PT, 0, c->stream>>>(c->arr[MHDGPU_DUDX], c->arr[MHDGPU_DUDY],
+                                             c->arr[MHDGPU_DIVB], plane, c->dred);
+    MHD_CHECK_LAUNCH();
+    reduce_final_kernel<<<1, 32, 0, c->stream>>>(c->dred, g, 1, 0, c->dscal + 3);
+    MHD_CHECK_LAUNCH();
+    MHD_CUDA_TRY(cudaMemcpyAsync(out, c->dscal + 3, sizeof(double), cudaMemcpyDeviceToHost,
+                                 c->stream));
+    MHD_CUDA_TRY(cudaStreamSynchronize(c->stream));
+    return MHDGPU_OK;
+}
+
+int launch_diagnostics(Ctx *c, double *energy, double *ch, int *finite)
+{
+    long plane = c->nx * c->ny;
+    int g = grid_for(c, plane);
+    if (3 * g > c->nred) g = c->nred / 3;
+    diag_kernel<<<g, PT, 0, c->stream>>>(c->arr[MHDGPU_UU], plane, c->p.adiabaticIdx, c->dred);
+    MHD_CHECK_LAUNCH();
+    reduce_final_kernel<<<1, 32, 0, c->stream>>>(c->dred, g, 3, 1, c->dscal + 4);
+    MHD_CHECK_LAUNCH();
+    double h[3];
+    MHD_CUDA_TRY(cudaMemcpyAsync(h, c->dscal + 4, sizeof h, cudaMemcpyDeviceToHost, c->stream));
+    MHD_CUDA_TRY(cudaStreamSynchronize(c->stream));
+    if (energy) *energy = h[0] * c->dx * c->dy;
+    if (ch) *ch = h[1] * c->dx * c->dy;
+    if (finite) *finite = h[2] == 0.0;
+    return MHDGPU_OK;
+}
+
+}  // namespace mhd
