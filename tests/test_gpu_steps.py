@@ -34,7 +34,8 @@ def test_orszag_tang_1_step_vs_reference(reference, di):
         d.steps(1, 1e-3)
         gu = d.get("uu")
         assert rel_l2(gu, ru).max() < STEP1_TOL
-        assert d.checkDivB() == pytest.approx(rdiv, rel=1e-9, abs=1e-14)
+        # a small difference of O(1) derivatives: compared on their scale
+        assert d.checkDivB() == pytest.approx(rdiv, rel=1e-9, abs=1e-12)
         assert O.energy(p, gu) == pytest.approx(O.energy(p, ru), rel=1e-12)
         assert O.cross_helicity(p, gu) == pytest.approx(O.cross_helicity(p, ru), rel=1e-12, abs=1e-14)
 
@@ -67,7 +68,7 @@ def test_divb_cleaning_modes_vs_reference(reference, cleaning):
     p, uu = ic.orszag_tang(64, 32, di=0.05, divBcleaning=cleaning)
     if cleaning == 2:
         rng = np.random.default_rng(7)
-        uu = np.concatenate([uu, 1e-3 * rng.standard_normal((1,) + uu.shape[1:])])
+        uu[8] = 1e-3 * rng.standard_normal(uu.shape[1:])
     ru, _, _ = run_ref(reference, p, uu, 2, 1e-3)
     with Domain(p, uu) as d:
         d.steps(2, 1e-3)

@@ -1,0 +1,131 @@
+"""CPU: the numpy oracle pinned against the reference.
+
+1. Golden fixtures (tests/golden/*.npz) written by the reference's own C code
+   (tests/golden/make_golden.py): every operator and whole steps.
+2. The live reference build (oracle/_ref/libmhdref.so) where present.
+3. Known-answer tests of the schemes (the reference ships no tests; these
+   restate properties of its numerics).
+"""
+import glob
+import math
+import os
+
+import numpy as np
+import pytest
+
+import mhd_oracle as O
+from conftest import ROOT, rel_l2
+from mhd2dcfdfftw_open_b200.config import InputParams
+
+GOLDEN = os.path.join(ROOT, "tests", "golden")
+
+
+def load(path):
+    z = np.load(path)
+    pd = {k[2:]: z[k].item() for k in z.files if k.startswith("p_")}
+    return z, InputParams(**pd)
+
+
+@pytest.mark.parametrize("path", sorted(glob.glob(os.path.join(GOLDEN, "ops_*.npz"))))
+def test_operators_match_golden(path):
+    z, p = load(path)
+    uu = z["uu"]
+    # the finite-difference parts reproduce the reference to the last bit
+    assert np.array_equal(O.derivX(uu, p.dx), z["derivX"])
+    assert np.array_equal(O.derivXX(uu, p.dx), z["derivXX"])
+    assert rel_l2(O.derivY(uu, p.Ly), z["derivY"]).max() < 1e-14
+    assert rel_l2(O.derivYY(uu, p.Ly), z["derivYY"]).max() < 1e-14
+    assert rel_l2(O.filtering(uu), z["filtering"]).max() < 1e-14
+    dt, _, _ = O.calcDt(p, uu, 0.0)
+    assert dt == float(z["calcDt"])
+
+
+@pytest.mark.parametrize("path", sorted(glob.glob(os.path.join(GOLDEN, "steps_*.npz"))))
+def test_steps_match_golden(path):
+    z, p = load(path)
+    for key in z.files:
+        if not key.startswith("uu_"):
+            continue
+        n = int(key[3:])
+        s = O.State(p, z["uu0"])
+        dt = O.steps(s, n, float(z["dt_fixed"]))
+        assert rel_l2(s.uu, z[key]).max() < 1e-13, (path, n)
+        assert dt == pytest.approx(float(z[f"dt_{n}"]), rel=1e-14)
+        # max|div B| is a small difference of O(1) derivatives: compare it on
+        # the derivatives' scale
+        assert O.check_divb(s) == pytest.approx(float(z[f"maxdivb_{n}"]), rel=1e-9, abs=1e-12)
+
+
+def test_oracle_matches_live_reference(reference):
+    from mhd2dcfdfftw_open_b200 import ic
+    p, uu = ic.orszag_tang(48, 32, di=0.05)
+    reference.setup(p)
+    reference.set_state(uu)
+    reference.steps(4, 1e-3)
+    s = O.State(p, uu)
+    O.steps(s, 4, 1e-3)
+    assert rel_l2(s.uu, reference.uu).max() < 1e-13
+
+
+# --- known-answer tests of the numerics ------------------------------------
+def test_compact_derivative_orders():
+    """8th-order interior, 4th-order edge rows: halving dx shrinks the
+    interior error by ~2^8 and the edge-row error by ~2^4."""
+    errs_in, errs_edge = [], []
+    for n in (32, 64):
+        L = 2 * math.pi
+        dx = L / n
+        x = np.arange(n) * dx
+        f = np.sin(3 * x)[:, None]
+        d = O.deriv_cfd1(f, dx)[:, 0]
+        e = np.abs(d - 3 * np.cos(3 * x))
+        errs_in.append(e[n // 2])
+        errs_edge.append(max(e[0], e[-1]))
+    # interior error is dominated by the edge rows' influence, which decays
+    assert errs_edge[0] / errs_edge[1] > 12  # ~16 for 4th order
+    assert errs_in[1] < errs_edge[1]
+
+
+def test_spectral_derivative_exact_for_trig_polynomials():
+    ny, Ly = 64, 3.0
+    y = np.arange(ny) * Ly / ny
+    k = 2 * math.pi / Ly
+    f = (np.sin(5 * k * y) + 0.5 * np.cos(11 * k * y))[None, None, :]
+    df = O.derivY(f, Ly)[0, 0]
+    assert np.abs(df - (5 * k * np.cos(5 * k * y) - 5.5 * k * np.sin(11 * k * y))).max() < 1e-12
+    d2 = O.derivYY(f, Ly)[0, 0]
+    assert np.abs(d2 + (25 * k * k * np.sin(5 * k * y) + 60.5 * k * k * np.cos(11 * k * y))).max() < 1e-10
+
+
+def test_filter_transfer_functions():
+    a, b, c, d = O.aInnerF, O.bInnerF, O.cInnerF, O.dInnerF
+    w = math.pi
+    T = (a + b * math.cos(w) + c * math.cos(2 * w) + d * math.cos(3 * w)) / (1 + 2 * O.alphaInnerF * math.cos(w))
+    assert abs(T) < 1e-14
+    assert abs(O.filt_y(64)[32]) < 1e-14
+    assert O.filt_y(64)[0] == pytest.approx(1.0, abs=1e-15)
+
+
+def test_rk3_order_on_linear_ode():
+    lam = -1.3
+    errs = []
+    for nsteps in (20, 40):
+        dt = 1.0 / nsteps
+        u = np.array([[[1.0]]])
+        rk = np.zeros_like(u)
+        for _ in range(nsteps):
+            rk[:] = 0
+            for i in range(3):
+                u, rk = O.rkExecute(u, lam * u, rk, i, dt)
+        errs.append(abs(u.item() - math.exp(lam)))
+    assert errs[0] / errs[1] > 7.0  # third order: ~8
+
+
+def test_uniform_state_is_stationary():
+    from mhd2dcfdfftw_open_b200 import ic
+    p, uu = ic.orszag_tang(16, 16)
+    uu[:] = 0
+    uu[0], uu[4], uu[7] = 2.0, 0.7, 1.1
+    s = O.State(p, uu)
+    O.steps(s, 2, 1e-3)
+    assert np.abs(s.uu - uu).max() < 1e-13
