@@ -1,0 +1,350 @@
+"""Benchmark of the RK3 step of the 2-D MHD solver on B200.
+
+Metric: cell-updates/s (nx*ny*steps / s; one update = one full RK3 step:
+three stages including the compact/spectral filter), FP64.
+
+Default workload: Alfvenic turbulence on a 4096 x 4096 periodic grid
+(box 20pi x 20pi, rho = 1, B0 = 1 along x, beta = 0.5, d_i = 0.1,
+eta = nu = 2e-4, dt = 2e-4), the configuration the reference's headline metric
+is quoted on; synthetic seeded initial condition (seed 1).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+N > 1 runs under torchrun, one process per GPU, each advancing its own
+replica of the domain (the whole domain lives on one GPU: replicas only, no
+collective on the data path); the timing is the max over ranks.
+
+`--impl reference` times the reference's own C implementation of the path
+(compiled from its sources into oracle/_ref/mhd_ref) on the host cores:
+P independent single-rank processes, each step a bounded sample (1024 x 1024
+turbulence, one RK3 step per process).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "cell-updates/s"
+UNIT = "cell-updates/s"
+DT = 2e-4
+
+
+def env_rank():
+    return (int(os.environ.get("RANK", "0")), int(os.environ.get("LOCAL_RANK", "0")),
+            int(os.environ.get("WORLD_SIZE", "1")))
+
+
+def measured_peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons, sampled every 200 ms while the
+    timed region runs."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index):
+        self.idx = device_index
+        self.proc = None
+        self.out = None
+
+    def start(self):
+        try:
+            self.out = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.idx), f"--query-gpu={self.QUERY}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=self.out, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.out.flush()
+        self.out.seek(0)
+        rows = [ln.split(",") for ln in self.out.read().splitlines() if ln.strip()]
+        os.unlink(self.out.name)
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            try:
+                sm.append(float(r[1]))
+                smax = float(r[2])
+                for k, nm in enumerate(names):
+                    if r[5 + k].strip().lower() == "active":
+                        reasons.add(nm)
+            except (ValueError, IndexError):
+                continue
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ---------------------------------------------------------------------------
+# the reference's CPU path (oracle/_ref/mhd_ref), bounded samples
+# ---------------------------------------------------------------------------
+CPU_SAMPLE = (1024, 1024)
+
+
+def cpu_processes():
+    n = os.cpu_count() or 1
+    return max(1, min(n, 32))
+
+
+def run_reference_sample(nsteps, warmup, nproc, timeout=600):
+    """nproc concurrent single-rank reference processes, each running warmup +
+    nsteps RK3 steps of the 1024^2 turbulence sample; returns
+    (aggregate cell-updates/s, max seconds, per-process results)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import ref  # the checker's build of the reference (test infrastructure)
+    from mhd2dcfdfftw_open_b200 import ic
+    from mhd2dcfdfftw_open_b200.dumpio import write_state
+
+    if not os.path.exists(ref.BIN_PATH):
+        raise RuntimeError("oracle/_ref/mhd_ref is not built")
+    nx, ny = CPU_SAMPLE
+    p, uu = ic.alfvenic_turbulence(nx, ny)
+    with tempfile.TemporaryDirectory(prefix="mhdcpu_") as wd:
+        p.write(os.path.join(wd, "input"))
+        icp = os.path.join(wd, "ic.dat")
+        write_state(icp, uu)
+        procs = [subprocess.Popen([ref.BIN_PATH, wd, icp, str(nsteps), repr(DT), "-", str(warmup)],
+                                  stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+                 for _ in range(nproc)]
+        res = []
+        for pr in procs:
+            out, _ = pr.communicate(timeout=timeout)
+            line = [ln for ln in out.splitlines() if ln.startswith("{")][-1]
+            res.append(json.loads(line))
+    tmax = max(r["seconds"] for r in res)
+    agg = nproc * nx * ny * nsteps / tmax
+    return agg, tmax, res
+
+
+# ---------------------------------------------------------------------------
+# our arm
+# ---------------------------------------------------------------------------
+def algorithmic_model_bytes():
+    """Minimal-pass FP64 traffic model of one cell-update (one RK3 step):
+    per stage, x pass 8 read + 16 written, y pass 32 read + 16 written, x and
+    y filters 16 each: 104 doubles = 832 B per stage, 2496 B per step."""
+    return 2496.0
+
+
+def traffic_per_launch(kclass):
+    """dram bytes per launch of a kernel class from the committed ncu summary
+    (profiles/ncu_traffic.json), or None."""
+    path = os.path.join(ROOT, "profiles", "ncu_traffic.json")
+    try:
+        with open(path) as f:
+            return float(json.load(f)[kclass]["dram_bytes_per_launch"])
+    except Exception:
+        return None
+
+
+def run_ours(args):
+    rank, local, world = env_rank()
+    import numpy as np
+    import torch
+
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+    from mhd2dcfdfftw_open_b200 import ic
+    from mhd2dcfdfftw_open_b200.solver import Domain
+
+    nx, ny = args.nx, args.ny
+    p, uu = ic.alfvenic_turbulence(nx, ny)
+    fused = args.path == "fused"
+    dom = Domain(p, uu, device=local)
+    stream = torch.cuda.ExternalStream(dom.stream_handle(), device=local)
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    # warm-up steps (untimed)
+    dom.steps(args.warmup, DT, fused=fused)
+    barrier()
+    torch.cuda.synchronize()
+    dom.synchronize()
+
+    sampler = ClockSampler(local)
+    sampler.start()
+    dom.profile(True)
+    l0 = dom.launch_count()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    dom.steps(args.steps, DT, fused=fused)
+    e1.record(stream)
+    e1.synchronize()
+    torch.cuda.synchronize()
+    barrier()
+    clocks = sampler.stop()
+    launches = dom.launch_count() - l0
+    ms = e0.elapsed_time(e1)
+    prof = dom.profile_read()
+    dom.profile(False)
+    if dist is not None:
+        t = torch.tensor([ms], dtype=torch.float64, device=f"cuda:{local}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    cells = float(nx) * ny
+    value = world * cells * args.steps / (ms / 1e3)
+
+    # end to end through the C ABI with host buffers: every step uploads the
+    # state from pinned host memory, advances one RK3 step and reads the state
+    # back into pinned host memory
+    ke = max(1, min(args.steps, args.e2e_steps))
+    h_in = torch.from_numpy(np.ascontiguousarray(dom.get("uu"))).pin_memory()
+    h_out = torch.empty_like(h_in).pin_memory()
+    nin, nout = h_in.numpy(), h_out.numpy()
+    dom.set("uu", nin)
+    dom.steps(1, DT, fused=fused)
+    barrier()
+    t0 = time.perf_counter()
+    for _ in range(ke):
+        dom.set("uu", nin)
+        dom.steps(1, DT, fused=fused)
+        dom.get("uu", out=nout)
+    t_e2e = time.perf_counter() - t0
+    if dist is not None:
+        t = torch.tensor([t_e2e], dtype=torch.float64, device=f"cuda:{local}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        t_e2e = float(t.item())
+    e2e = world * cells * ke / t_e2e
+    nbytes = nin.nbytes
+    dom.close()
+
+    if rank != 0:
+        if dist is not None:
+            dist.destroy_process_group()
+        return
+    peak, peak_kind = measured_peaks()
+    dom_cls = max(prof, key=lambda k: prof[k][0])
+    tot_ms, nl, byts = prof[dom_cls]
+    achieved = byts / (tot_ms / 1e3) / 1e9 if tot_ms > 0 else 0.0
+    tr = traffic_per_launch(dom_cls)
+    roofline = {"kernel": dom_cls, "bound": "hbm", "achieved": round(achieved, 1),
+                "peak": peak, "peak_kind": peak_kind, "unit": "GB/s",
+                "frac": round(achieved / peak, 4),
+                "traffic": tr,
+                "algorithmic_bytes_per_launch": byts / max(nl, 1),
+                "avg_launch_ms": tot_ms / max(nl, 1), "launches": nl,
+                "share_of_step": round(tot_ms / ms, 3)}
+    out = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64", "data": "synthetic (seeded Alfvenic turbulence IC, seed 1)",
+        "config": {"workload": f"alfvenic_turbulence_{nx}x{ny}_fp64", "nx": nx, "ny": ny,
+                   "dt": DT, "path": args.path, "parallelism": f"replicas{world}",
+                   "l2": "inputs larger than L2 (state alone is "
+                         f"{8 * cells * 8 / 1e9:.2f} GB)"},
+        "roofline": roofline,
+        "model_fraction": {"bytes_per_cell_update": algorithmic_model_bytes(),
+                           "frac": round(value / world * algorithmic_model_bytes() / (peak * 1e9), 4)},
+        "kernel_classes": {k: {"ms": round(v[0], 3), "launches": v[1]} for k, v in prof.items() if v[1]},
+        "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": nbytes,
+                "d2h_bytes_per_step": nbytes, "steps": ke},
+        "gpu_launches": launches,
+        "clocks": clocks,
+    }
+    if world == 1 and not args.no_cpu_baseline:
+        try:
+            nproc = cpu_processes()
+            agg, tmax, _ = run_reference_sample(1, 0, nproc)
+            out["cpu_baseline"] = {"value": agg, "unit": UNIT, "cores": nproc, "kind": "reference",
+                                   "sample": f"turbulence {CPU_SAMPLE[0]}x{CPU_SAMPLE[1]}, 1 RK3 step "
+                                             f"in each of {nproc} independent single-rank "
+                                             f"processes ({tmax:.1f} s)"}
+        except Exception as e:  # reported, not hidden
+            out["cpu_baseline"] = {"value": None, "error": str(e)[:200]}
+    print(json.dumps(out), flush=True)
+    if dist is not None:
+        dist.destroy_process_group()
+
+
+# ---------------------------------------------------------------------------
+# reference arm
+# ---------------------------------------------------------------------------
+def run_reference(args):
+    rank, _, world = env_rank()
+    if rank != 0:
+        return
+    global CPU_SAMPLE
+    n = args.steps + args.warmup
+    CPU_SAMPLE = (1024, 1024) if n <= 20 else ((512, 512) if n <= 80 else (256, 256))
+    nproc = cpu_processes()
+    agg, tmax, _ = run_reference_sample(args.steps, args.warmup, nproc)
+    sample = (f"turbulence {CPU_SAMPLE[0]}x{CPU_SAMPLE[1]} per step, {nproc} independent "
+              "single-rank processes of the reference's C code (oracle/_ref/mhd_ref)")
+    out = {
+        "metric": METRIC, "value": agg, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": tmax * 1e3 / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded Alfvenic turbulence IC, seed 1)",
+        "config": {"workload": f"alfvenic_turbulence_{args.nx}x{args.ny}_fp64", "nx": args.nx,
+                   "ny": args.ny, "dt": DT, "sample": sample},
+        "impl": "reference",
+        "cpu_baseline": {"value": agg, "unit": UNIT, "cores": nproc, "kind": "reference",
+                         "sample": sample},
+        "e2e": {"value": agg, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(out), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--path", choices=["fused", "operators"], default="fused")
+    ap.add_argument("--nx", type=int, default=4096)
+    ap.add_argument("--ny", type=int, default=4096)
+    ap.add_argument("--e2e-steps", type=int, default=5)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -120,6 +120,22 @@ int mhdgpu_steps_fused(mhdgpu_ctx *ctx, int nsteps, double dt_fixed, double *dt_
 int mhdgpu_diagnostics(mhdgpu_ctx *ctx, double *energy, double *cross_helicity,
                        int *finite);
 
+/* --- instrumentation ---------------------------------------------------- */
+/* the context's CUDA stream (a cudaStream_t), for callers that time or order
+ * work around the library's launches */
+void *mhdgpu_stream(mhdgpu_ctx *ctx);
+/* number of kernels this context has launched so far */
+long mhdgpu_launch_count(const mhdgpu_ctx *ctx);
+/* enable (1) / disable (0) CUDA-event bracketing of every launch; enabling
+ * clears the record */
+int mhdgpu_profile(mhdgpu_ctx *ctx, int enable);
+/* total device time, launch count and algorithmic bytes (what the launches
+ * must read and write at least) recorded for a kernel class:
+ * 0 x-line solver, 1 y spectral, 2 pointwise, 3 reductions,
+ * 4 fused x pass, 5 fused y pass */
+int mhdgpu_profile_read(mhdgpu_ctx *ctx, int kclass, double *total_ms, long *count,
+                        double *bytes);
+
 #ifdef __cplusplus
 }
 #endif

@@ -108,6 +108,11 @@ extern "C" void mhdgpu_destroy(mhdgpu_ctx *h)
     cudaFree(c->dscal);
     cudaFree(c->dred);
     cudaFree(c->dflag);
+    if (c->prof_ev) {
+        for (int i = 0; i < 2 * MHD_PROF_MAX; i++) cudaEventDestroy(c->prof_ev[i]);
+        free(c->prof_ev);
+        free(c->prof_cls);
+    }
     if (c->stream) cudaStreamDestroy(c->stream);
     delete c;
 }
@@ -411,4 +416,73 @@ extern "C" int mhdgpu_diagnostics(mhdgpu_ctx *h, double *energy, double *cross_h
 {
     CTX_OR_FAIL(h);
     return mhd::launch_diagnostics(c, energy, cross_helicity, finite);
+}
+
+// ---------------------------------------------------------------------------
+// instrumentation
+// ---------------------------------------------------------------------------
+void prof_begin(Ctx *c, int kclass, double bytes)
+{
+    c->launches++;
+    if (!c->prof_on || c->prof_n >= MHD_PROF_MAX) return;
+    c->prof_bytes[kclass] += bytes;
+    c->prof_cls[c->prof_n] = kclass;
+    cudaEventRecord(c->prof_ev[2 * c->prof_n], c->stream);
+}
+
+void prof_end(Ctx *c)
+{
+    if (!c->prof_on || c->prof_n >= MHD_PROF_MAX) return;
+    cudaEventRecord(c->prof_ev[2 * c->prof_n + 1], c->stream);
+    c->prof_n++;
+}
+
+extern "C" void *mhdgpu_stream(mhdgpu_ctx *h)
+{
+    Ctx *c = reinterpret_cast<Ctx *>(h);
+    return c ? (void *)c->stream : nullptr;
+}
+
+extern "C" long mhdgpu_launch_count(const mhdgpu_ctx *h)
+{
+    const Ctx *c = reinterpret_cast<const Ctx *>(h);
+    return c ? c->launches : -1;
+}
+
+extern "C" int mhdgpu_profile(mhdgpu_ctx *h, int enable)
+{
+    CTX_OR_FAIL(h);
+    if (enable && !c->prof_ev) {
+        c->prof_ev = (cudaEvent_t *)calloc(2 * MHD_PROF_MAX, sizeof(cudaEvent_t));
+        c->prof_cls = (int *)calloc(MHD_PROF_MAX, sizeof(int));
+        if (!c->prof_ev || !c->prof_cls) return mhd_set_error(MHDGPU_ERR_NOMEM);
+        for (int i = 0; i < 2 * MHD_PROF_MAX; i++)
+            MHD_CUDA_TRY(cudaEventCreate(&c->prof_ev[i]));
+    }
+    c->prof_on = enable ? 1 : 0;
+    if (enable) {
+        c->prof_n = 0;
+        for (int k = 0; k < 8; k++) c->prof_bytes[k] = 0.0;
+    }
+    return MHDGPU_OK;
+}
+
+extern "C" int mhdgpu_profile_read(mhdgpu_ctx *h, int kclass, double *total_ms, long *count,
+                                   double *bytes)
+{
+    CTX_OR_FAIL(h);
+    MHD_CUDA_TRY(cudaStreamSynchronize(c->stream));
+    double tot = 0.0;
+    long n = 0;
+    for (int i = 0; i < c->prof_n; i++) {
+        if (c->prof_cls[i] != kclass) continue;
+        float ms = 0.f;
+        MHD_CUDA_TRY(cudaEventElapsedTime(&ms, c->prof_ev[2 * i], c->prof_ev[2 * i + 1]));
+        tot += ms;
+        n++;
+    }
+    if (total_ms) *total_ms = tot;
+    if (count) *count = n;
+    if (bytes) *bytes = (kclass >= 0 && kclass < 8) ? c->prof_bytes[kclass] : 0.0;
+    return MHDGPU_OK;
 }

@@ -41,6 +41,11 @@ struct XTables {
 };
 
 #define MHD_MAX_CLUSTER 16
+#define MHD_PROF_MAX 8192
+
+// kernel classes for the event-timing hooks (mhdgpu_profile_read)
+enum KClass { KC_XSOLVE = 0, KC_YSPEC, KC_POINTWISE, KC_REDUCE, KC_FUSED_X, KC_FUSED_Y,
+              KC_NCLASS };
 
 struct Ctx {
     mhdgpu_params p;
@@ -74,6 +79,13 @@ struct Ctx {
     double *yscr;                // per-CTA row scratch of the fused y pass
     long yscr_rows;
     int fused_pending_filter;    // 1: uu still needs the x filter
+    // instrumentation: launch counter and per-kernel-class event timing
+    long launches;
+    int prof_on;
+    int prof_n;
+    cudaEvent_t *prof_ev;        // 2 * MHD_PROF_MAX events (begin, end)
+    int *prof_cls;
+    double prof_bytes[8];        // algorithmic bytes of the profiled launches per class
 };
 
 }  // namespace mhd
@@ -88,6 +100,10 @@ int mhd_set_error(int status);
     } while (0)
 
 #define MHD_CHECK_LAUNCH() MHD_CUDA_TRY(cudaGetLastError())
+
+// Bracket a launch with events when profiling is on; always count it.
+void prof_begin(mhd::Ctx *c, int kclass, double bytes);
+void prof_end(mhd::Ctx *c);
 
 // kernels launched by api.cu, defined in the other translation units
 namespace mhd {

@@ -307,8 +307,10 @@ __global__ void reduce_final_kernel(const double *part, int nparts, int stride, 
 int launch_efield(Ctx *c)
 {
     long plane = c->nx * c->ny;
+    prof_begin(c, KC_POINTWISE, 9.0 * plane * 8.0);
     efield_kernel<<<grid_for(c, plane), PT, 0, c->stream>>>(c->arr[MHDGPU_UU],
                                                              c->arr[MHDGPU_EFIELD], plane);
+    prof_end(c);
     MHD_CHECK_LAUNCH();
     return MHDGPU_OK;
 }
@@ -316,10 +318,22 @@ int launch_efield(Ctx *c)
 int launch_divb(Ctx *c, double *out)
 {
     long plane = c->nx * c->ny;
+    prof_begin(c, KC_POINTWISE, 3.0 * plane * 8.0);
     divb_kernel<<<grid_for(c, plane), PT, 0, c->stream>>>(c->arr[MHDGPU_DUDX], c->arr[MHDGPU_DUDY],
                                                            out, plane);
+    prof_end(c);
     MHD_CHECK_LAUNCH();
     return MHDGPU_OK;
+}
+
+// fields calcRHS reads and writes
+static int rhs_fields(const Ctx *c)
+{
+    int n = 3 * c->nvar + 2 + 2 + c->nvar;  // uu, dudx, dudy, dEdx(Ey,Ez), dEdy(Ex,Ez), dudt
+    if (c->p.viscosity > 0) n += 6;
+    if (c->p.resistivity > 0) n += 6;
+    if (c->p.divBcleaning == 1) n += 2;
+    return n;
 }
 
 int launch_rhs(Ctx *c)
@@ -345,7 +359,9 @@ int launch_rhs(Ctx *c)
     a.Ch = c->Ch;
     a.Cp = c->Cp;
     a.cleaning = c->p.divBcleaning;
+    prof_begin(c, KC_POINTWISE, (double)rhs_fields(c) * a.plane * 8.0);
     rhs_kernel<<<grid_for(c, a.plane), PT, 0, c->stream>>>(a);
+    prof_end(c);
     MHD_CHECK_LAUNCH();
     return MHDGPU_OK;
 }
@@ -353,9 +369,11 @@ int launch_rhs(Ctx *c)
 int launch_rk(Ctx *c, int iRK)
 {
     long n = (long)c->nvar * c->nx * c->ny;
+    prof_begin(c, KC_POINTWISE, 5.0 * n * 8.0);
     rk_kernel<<<grid_for(c, n), PT, 0, c->stream>>>(c->arr[MHDGPU_UU], c->arr[MHDGPU_DUDT],
                                                      c->arr[MHDGPU_DUDTRK], n, c->cc[iRK],
                                                      c->dd[iRK]);
+    prof_end(c);
     MHD_CHECK_LAUNCH();
     return MHDGPU_OK;
 }
@@ -376,9 +394,13 @@ int launch_calc_dt(Ctx *c, double dt0, double *dt_out)
     a.part = c->dred;
     int g = grid_for(c, a.plane);
     if (g > c->nred) g = c->nred;
+    prof_begin(c, KC_REDUCE, 7.0 * a.plane * 8.0);
     dt_partial_kernel<<<g, PT, 0, c->stream>>>(a);
+    prof_end(c);
     MHD_CHECK_LAUNCH();
+    prof_begin(c, KC_REDUCE, 0.0);
     dt_final_kernel<<<1, 1024, 0, c->stream>>>(a, g, c->p.cfl, dt0, c->p.divBcleaning, c->dscal);
+    prof_end(c);
     MHD_CHECK_LAUNCH();
     double h[3];
     MHD_CUDA_TRY(cudaMemcpyAsync(h, c->dscal, sizeof h, cudaMemcpyDeviceToHost, c->stream));
@@ -396,10 +418,14 @@ int launch_max_divb(Ctx *c, double *out)
     long plane = c->nx * c->ny;
     int g = grid_for(c, plane);
     if (g > c->nred) g = c->nred;
+    prof_begin(c, KC_REDUCE, 3.0 * plane * 8.0);
     maxdivb_kernel<<<g, PT, 0, c->stream>>>(c->arr[MHDGPU_DUDX], c->arr[MHDGPU_DUDY],
                                              c->arr[MHDGPU_DIVB], plane, c->dred);
+    prof_end(c);
     MHD_CHECK_LAUNCH();
+    prof_begin(c, KC_REDUCE, 0.0);
     reduce_final_kernel<<<1, 32, 0, c->stream>>>(c->dred, g, 1, 0, c->dscal + 3);
+    prof_end(c);
     MHD_CHECK_LAUNCH();
     MHD_CUDA_TRY(cudaMemcpyAsync(out, c->dscal + 3, sizeof(double), cudaMemcpyDeviceToHost,
                                  c->stream));
@@ -412,9 +438,13 @@ int launch_diagnostics(Ctx *c, double *energy, double *ch, int *finite)
     long plane = c->nx * c->ny;
     int g = grid_for(c, plane);
     if (3 * g > c->nred) g = c->nred / 3;
+    prof_begin(c, KC_REDUCE, 8.0 * plane * 8.0);
     diag_kernel<<<g, PT, 0, c->stream>>>(c->arr[MHDGPU_UU], plane, c->p.adiabaticIdx, c->dred);
+    prof_end(c);
     MHD_CHECK_LAUNCH();
+    prof_begin(c, KC_REDUCE, 0.0);
     reduce_final_kernel<<<1, 32, 0, c->stream>>>(c->dred, g, 3, 1, c->dscal + 4);
+    prof_end(c);
     MHD_CHECK_LAUNCH();
     double h[3];
     MHD_CUDA_TRY(cudaMemcpyAsync(h, c->dscal + 4, sizeof h, cudaMemcpyDeviceToHost, c->stream));

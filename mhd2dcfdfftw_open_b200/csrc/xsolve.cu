@@ -432,7 +432,9 @@ int launch_xsolve(Ctx *c, int op, int nv, const double *in, int in_start, double
     attr[0].val.clusterDim.z = 1;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
+    prof_begin(c, KC_XSOLVE, (double)c->nx * c->ny * 8.0 * (double)((src_kind ? 4 : nv) + nv));
     MHD_CUDA_TRY(cudaLaunchKernelEx(&cfg, xsolve_kernel, a));
+    prof_end(c);
     return MHDGPU_OK;
 }
 

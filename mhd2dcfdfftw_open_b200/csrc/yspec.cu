@@ -219,7 +219,9 @@ int launch_yspec(Ctx *c, int op, int nv, const double *in, int in_start, double 
     a.out_start = out_start;
     dim3 grid((unsigned)c->nx, (unsigned)((nv + 1) / 2), 1);
     int thr = (int)std::min<long>(YT, std::max<long>(32, c->ny / 4));
+    prof_begin(c, KC_YSPEC, (double)c->nx * c->ny * 8.0 * 2.0 * nv);
     yspec_kernel<<<grid, thr, sizeof(double2) * c->ny, c->stream>>>(a);
+    prof_end(c);
     MHD_CHECK_LAUNCH();
     return MHDGPU_OK;
 }

@@ -42,8 +42,12 @@ EXPORTED = (
     "mhdgpu_calc_efield", "mhdgpu_calc_divb", "mhdgpu_calc_rhs", "mhdgpu_rk_init",
     "mhdgpu_rk_execute", "mhdgpu_filtering", "mhdgpu_calc_dt", "mhdgpu_check_divb",
     "mhdgpu_get_cleaning_speeds", "mhdgpu_stage", "mhdgpu_steps", "mhdgpu_steps_fused",
-    "mhdgpu_diagnostics",
+    "mhdgpu_diagnostics", "mhdgpu_stream", "mhdgpu_launch_count", "mhdgpu_profile",
+    "mhdgpu_profile_read",
 )
+
+# kernel classes of mhdgpu_profile_read
+KCLASSES = ("xsolve", "yspec", "pointwise", "reduce", "fused_x", "fused_y")
 
 _lib = None
 
@@ -87,6 +91,12 @@ def load_library(path: str = LIB_PATH):
     L.mhdgpu_steps.argtypes = [vp, ctypes.c_int, ctypes.c_double, dp]
     L.mhdgpu_steps_fused.argtypes = [vp, ctypes.c_int, ctypes.c_double, dp]
     L.mhdgpu_diagnostics.argtypes = [vp, dp, dp, ctypes.POINTER(ctypes.c_int)]
+    L.mhdgpu_stream.argtypes = [vp]
+    L.mhdgpu_stream.restype = vp
+    L.mhdgpu_launch_count.argtypes = [vp]
+    L.mhdgpu_launch_count.restype = ctypes.c_long
+    L.mhdgpu_profile.argtypes = [vp, ctypes.c_int]
+    L.mhdgpu_profile_read.argtypes = [vp, ctypes.c_int, dp, ctypes.POINTER(ctypes.c_long), dp]
     _lib = L
     return L
 
@@ -144,9 +154,12 @@ class Domain:
         a = np.ascontiguousarray(arr, dtype=np.float64).reshape(n, self.p.nx, self.p.ny)
         self._check(self.lib.mhdgpu_set_array(self.h, which, _dptr(a)))
 
-    def get(self, name):
+    def get(self, name, out=None):
         which = ARRAY_NAMES[name]
-        a = np.empty((self._nfields(which), self.p.nx, self.p.ny))
+        shape = (self._nfields(which), self.p.nx, self.p.ny)
+        a = np.empty(shape) if out is None else out
+        if a.shape != shape or a.dtype != np.float64 or not a.flags.c_contiguous:
+            raise ValueError("out must be a C-contiguous float64 array of shape %s" % (shape,))
         self._check(self.lib.mhdgpu_get_array(self.h, which, _dptr(a)))
         return a
 
@@ -221,3 +234,25 @@ class Domain:
     @property
     def uu(self):
         return self.get("uu")
+
+    # -- instrumentation ---------------------------------------------------
+    def stream_handle(self) -> int:
+        """The context's cudaStream_t as an integer (for torch.cuda.ExternalStream)."""
+        return int(self.lib.mhdgpu_stream(self.h) or 0)
+
+    def launch_count(self) -> int:
+        return int(self.lib.mhdgpu_launch_count(self.h))
+
+    def profile(self, enable: bool):
+        self._check(self.lib.mhdgpu_profile(self.h, 1 if enable else 0))
+
+    def profile_read(self):
+        """{kernel class: (total ms, launches, algorithmic bytes)} of the
+        profiled launches."""
+        out = {}
+        for k, name in enumerate(KCLASSES):
+            ms, n, b = ctypes.c_double(), ctypes.c_long(), ctypes.c_double()
+            self._check(self.lib.mhdgpu_profile_read(self.h, k, ctypes.byref(ms), ctypes.byref(n),
+                                                     ctypes.byref(b)))
+            out[name] = (ms.value, n.value, b.value)
+        return out

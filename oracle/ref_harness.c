@@ -153,22 +153,24 @@ int ref_save_state(const char *path, double t)
 }
 
 #ifdef ORACLE_MAIN
-/* mhd_ref <workdir> <state.dat> <nsteps> <dt> [out.dat]
- * Runs nsteps RK3 steps of the reference from the given state (dt <= 0 uses
- * the reference's CFL control) and prints one JSON line with the step-loop
- * time.  Used as the CPU baseline. */
+/* mhd_ref <workdir> <state.dat> <nsteps> <dt> [out.dat [warmup]]
+ * Runs `warmup` untimed steps, then nsteps timed RK3 steps of the reference
+ * from the given state (dt <= 0 uses the reference's CFL control) and prints
+ * one JSON line with the timed step-loop seconds.  Used as the CPU baseline. */
 int main(int argc, char **argv)
 {
     if (argc < 5) {
-        fprintf(stderr, "usage: %s workdir state.dat nsteps dt [out.dat]\n", argv[0]);
+        fprintf(stderr, "usage: %s workdir state.dat nsteps dt [out.dat|- [warmup]]\n", argv[0]);
         return 2;
     }
     if (ref_setup(argv[1]) != 0) { fprintf(stderr, "setup failed\n"); return 1; }
     if (ref_load_state(argv[2]) != 0) { fprintf(stderr, "cannot read %s\n", argv[2]); return 1; }
     int nsteps = atoi(argv[3]);
+    int warm = argc > 6 ? atoi(argv[6]) : 0;
     double dt = atof(argv[4]), dtio = 0.0;
+    if (warm > 0) (void)ref_steps(warm, dt, &dtio);
     double sec = ref_steps(nsteps, dt, &dtio);
-    if (argc > 5) ref_save_state(argv[5], 0.0);
+    if (argc > 5 && strcmp(argv[5], "-") != 0) ref_save_state(argv[5], 0.0);
     double cells = (double)nx * (double)ny * (double)nsteps;
     printf("{\"nx\": %zu, \"ny\": %zu, \"steps\": %d, \"seconds\": %.6f, "
            "\"cell_updates_per_s\": %.6e, \"dt\": %.17g}\n",
