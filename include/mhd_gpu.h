@@ -120,6 +120,23 @@ int mhdgpu_steps_fused(mhdgpu_ctx *ctx, int nsteps, double dt_fixed, double *dt_
 int mhdgpu_diagnostics(mhdgpu_ctx *ctx, double *energy, double *cross_helicity,
                        int *finite);
 
+/* --- allocation-free time step ---------------------------------------------
+ * No counterpart in the reference.  The CFL time step of calcDt for callers
+ * that cannot allocate device memory (a framework whose pool allocator owns
+ * the device's memory, a service that fixes its footprint at start-up): no
+ * context, no allocation, no host synchronisation.  d_uu: the state
+ * [NVAR][nx][ny] on the current device; d_out: 3 device doubles receiving
+ * dt (after the 2% hysteresis against dt0), Ch and Cp (hyperbolic cleaning,
+ * else 0); stream: a cudaStream_t (NULL: the default stream), the call is
+ * asynchronous on it.  Scratch is a fixed 128 KiB device array held by every
+ * GPU that loads the library: nx*ny is limited to 33,554,432 cells, larger
+ * grids return MHDGPU_ERR_INVALID.  Calls share that array: calls that
+ * overlap on the GPU race and must be serialised by the caller.  The first
+ * call on a device looks the array up with that device current; make it
+ * before any stream capture begins. */
+int mhdgpu_calc_dt_noalloc(const double *d_uu, const mhdgpu_params *p, double dt0,
+                           double *d_out, void *stream);
+
 /* --- instrumentation ---------------------------------------------------- */
 /* the context's CUDA stream (a cudaStream_t), for callers that time or order
  * work around the library's launches */
