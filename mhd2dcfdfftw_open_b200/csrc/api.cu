@@ -193,6 +193,17 @@ extern "C" int mhdgpu_nvar(const mhdgpu_ctx *h)
     if (!c) return mhd_set_error(MHDGPU_ERR_INVALID);           \
     if (cudaSetDevice(c->device) != cudaSuccess) return mhd_set_error(MHDGPU_ERR_CUDA)
 
+namespace mhd {
+int fused_apply_pending_filter(Ctx *c);
+}
+
+// Apply the x filter that the fused stage leaves pending, so that every
+// public entry point sees the same state as the reference would hold.
+static int settle(Ctx *c)
+{
+    return c->fused_pending_filter ? mhd::fused_apply_pending_filter(c) : MHDGPU_OK;
+}
+
 extern "C" double *mhdgpu_device_array(mhdgpu_ctx *h, int which)
 {
     Ctx *c = reinterpret_cast<Ctx *>(h);
@@ -216,6 +227,7 @@ extern "C" int mhdgpu_set_array(mhdgpu_ctx *h, int which, const double *host)
 extern "C" int mhdgpu_get_array(mhdgpu_ctx *h, int which, double *host)
 {
     CTX_OR_FAIL(h);
+    if (which == MHDGPU_UU && settle(c)) return mhdgpu_last_error();
     if (which < 0 || which >= MHDGPU_NARRAYS || !host || !c->arr[which])
         return mhd_set_error(MHDGPU_ERR_INVALID);
     size_t n = (size_t)c->arr_fields[which] * c->nx * c->ny;
@@ -240,6 +252,7 @@ static int check_flag(Ctx *c)
 extern "C" int mhdgpu_synchronize(mhdgpu_ctx *h)
 {
     CTX_OR_FAIL(h);
+    if (settle(c)) return mhdgpu_last_error();
     MHD_CUDA_TRY(cudaStreamSynchronize(c->stream));
     return check_flag(c);
 }
@@ -256,6 +269,7 @@ static bool arr_ok(const Ctx *c, int which, int first, int nv)
 extern "C" int mhdgpu_deriv_x(mhdgpu_ctx *h, int nv, int in, int start, int out, int order)
 {
     CTX_OR_FAIL(h);
+    if (settle(c)) return mhdgpu_last_error();
     if (order != 1 && order != 2) return mhd_set_error(MHDGPU_ERR_INVALID);
     if (!arr_ok(c, in, start, nv) || !arr_ok(c, out, 0, nv)) return mhd_set_error(MHDGPU_ERR_INVALID);
     return mhd::launch_xsolve(c, order == 1 ? mhd::XOP_D1 : mhd::XOP_D2, nv, c->arr[in], start,
@@ -265,6 +279,7 @@ extern "C" int mhdgpu_deriv_x(mhdgpu_ctx *h, int nv, int in, int start, int out,
 extern "C" int mhdgpu_deriv_y(mhdgpu_ctx *h, int nv, int in, int start, int out, int order)
 {
     CTX_OR_FAIL(h);
+    if (settle(c)) return mhdgpu_last_error();
     if (order != 1 && order != 2) return mhd_set_error(MHDGPU_ERR_INVALID);
     if (!arr_ok(c, in, start, nv) || !arr_ok(c, out, 0, nv)) return mhd_set_error(MHDGPU_ERR_INVALID);
     return mhd::launch_yspec(c, order - 1, nv, c->arr[in], start, c->arr[out], 0);
@@ -273,6 +288,7 @@ extern "C" int mhdgpu_deriv_y(mhdgpu_ctx *h, int nv, int in, int start, int out,
 extern "C" int mhdgpu_calc_efield(mhdgpu_ctx *h)
 {
     CTX_OR_FAIL(h);
+    if (settle(c)) return mhdgpu_last_error();
     return mhd::launch_efield(c);
 }
 
@@ -285,6 +301,7 @@ extern "C" int mhdgpu_calc_divb(mhdgpu_ctx *h)
 extern "C" int mhdgpu_calc_rhs(mhdgpu_ctx *h)
 {
     CTX_OR_FAIL(h);
+    if (settle(c)) return mhdgpu_last_error();
     return mhd::launch_rhs(c);
 }
 
@@ -307,6 +324,7 @@ extern "C" int mhdgpu_rk_init(mhdgpu_ctx *h, double dt)
 extern "C" int mhdgpu_rk_execute(mhdgpu_ctx *h, int iRK)
 {
     CTX_OR_FAIL(h);
+    if (settle(c)) return mhdgpu_last_error();
     if (iRK < 0 || iRK > 2) return mhd_set_error(MHDGPU_ERR_INVALID);
     return mhd::launch_rk(c, iRK);
 }
@@ -316,6 +334,7 @@ extern "C" int mhdgpu_rk_execute(mhdgpu_ctx *h, int iRK)
 extern "C" int mhdgpu_filtering(mhdgpu_ctx *h)
 {
     CTX_OR_FAIL(h);
+    if (settle(c)) return mhdgpu_last_error();
     int rc = mhd::launch_xsolve(c, mhd::XOP_F, c->nvar, c->arr[MHDGPU_UU], 0, c->arr[MHDGPU_UU], 0);
     if (rc) return rc;
     return mhd::launch_yspec(c, 2, c->nvar, c->arr[MHDGPU_UU], 0, c->arr[MHDGPU_UU], 0);
@@ -324,6 +343,7 @@ extern "C" int mhdgpu_filtering(mhdgpu_ctx *h)
 extern "C" int mhdgpu_calc_dt(mhdgpu_ctx *h, double dt0, double *dt_out)
 {
     CTX_OR_FAIL(h);
+    if (settle(c)) return mhdgpu_last_error();
     return mhd::launch_calc_dt(c, dt0, dt_out);
 }
 
@@ -357,7 +377,7 @@ extern "C" int mhdgpu_stage(mhdgpu_ctx *h, int iRK)
 {
     CTX_OR_FAIL(h);
     if (iRK < 0 || iRK > 2) return mhd_set_error(MHDGPU_ERR_INVALID);
-    if (c->fused_pending_filter) return mhd_set_error(MHDGPU_ERR_INVALID);
+    TRY(settle(c));
     const mhdgpu_params &p = c->p;
     TRY(mhdgpu_deriv_x(h, c->nvar, MHDGPU_UU, 0, MHDGPU_DUDX, 1));
     TRY(mhdgpu_deriv_y(h, c->nvar, MHDGPU_UU, 0, MHDGPU_DUDY, 1));
@@ -399,6 +419,7 @@ extern "C" int mhdgpu_steps(mhdgpu_ctx *h, int nsteps, double dt_fixed, double *
 {
     CTX_OR_FAIL(h);
     if (nsteps < 0) return mhd_set_error(MHDGPU_ERR_INVALID);
+    TRY(settle(c));
     double dt = dt_io ? *dt_io : 0.0;
     TRY(next_dt(h, c, dt_fixed, &dt));
     TRY(mhdgpu_rk_init(h, dt));
@@ -412,9 +433,35 @@ extern "C" int mhdgpu_steps(mhdgpu_ctx *h, int nsteps, double dt_fixed, double *
     return check_flag(c);
 }
 
+// Steps through the fused stage (fused.cu).  Diffusive cleaning
+// (divBcleaning == 1) needs d/dx, d/dy of divB inside the stage and runs
+// through the operator stage instead.
+extern "C" int mhdgpu_steps_fused(mhdgpu_ctx *h, int nsteps, double dt_fixed, double *dt_io)
+{
+    CTX_OR_FAIL(h);
+    if (nsteps < 0) return mhd_set_error(MHDGPU_ERR_INVALID);
+    if (c->p.divBcleaning == 1) return mhdgpu_steps(h, nsteps, dt_fixed, dt_io);
+    const bool need_dt = dt_fixed <= 0 || c->p.divBcleaning == 2;
+    double dt = dt_io ? *dt_io : 0.0;
+    if (need_dt) TRY(settle(c));
+    TRY(next_dt(h, c, dt_fixed, &dt));
+    TRY(mhdgpu_rk_init(h, dt));
+    for (int s = 0; s < nsteps; s++) {
+        for (int k = 0; k < 3; k++) TRY(mhd::fused_stage(c, k, s == 0 && k == 0, k == 2));
+        if (need_dt) TRY(settle(c));
+        TRY(next_dt(h, c, dt_fixed, &dt));
+        TRY(mhdgpu_rk_init(h, dt));
+    }
+    TRY(settle(c));
+    if (dt_io) *dt_io = dt;
+    MHD_CUDA_TRY(cudaStreamSynchronize(c->stream));
+    return check_flag(c);
+}
+
 extern "C" int mhdgpu_diagnostics(mhdgpu_ctx *h, double *energy, double *cross_helicity, int *finite)
 {
     CTX_OR_FAIL(h);
+    if (settle(c)) return mhdgpu_last_error();
     return mhd::launch_diagnostics(c, energy, cross_helicity, finite);
 }
 

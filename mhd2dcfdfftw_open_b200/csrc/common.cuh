@@ -86,6 +86,10 @@ struct Ctx {
     cudaEvent_t *prof_ev;        // 2 * MHD_PROF_MAX events (begin, end)
     int *prof_cls;
     double prof_bytes[8];        // algorithmic bytes of the profiled launches per class
+    // fused x pass: Thomas factor edge tables and interior constants, tiling
+    double *xf_edge;
+    double xf_inner[2][3];
+    int xf_W, xf_C, xf_R;
 };
 
 }  // namespace mhd
@@ -122,6 +126,8 @@ int launch_rk(Ctx *c, int iRK);
 int launch_calc_dt(Ctx *c, double dt0, double *dt_out);
 int launch_max_divb(Ctx *c, double *out);
 int launch_diagnostics(Ctx *c, double *energy, double *ch, int *finite);
+int xfused_setup(Ctx *c);
+void xfused_free(Ctx *c);
 int fused_setup(Ctx *c);
 void fused_free(Ctx *c);
 int fused_stage(Ctx *c, int iRK, int first_stage_of_run, int last_stage);

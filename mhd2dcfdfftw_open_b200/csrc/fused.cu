@@ -1,19 +1,101 @@
-// Fused two-pass RK3 stage (x pass + y pass); filled in below the operator
-// path.
+// Fused RK3 stage: the reference's stage (mhd.c:154-199) regrouped into an x
+// pass and a y pass.
+//
+// The x filter and the y filter act on different axes and commute, so the
+// stage's closing filter F_y(F_x(u)) is applied as F_x(F_y(u)): the y filter
+// closes the y pass of stage k, and the x filter opens the x pass of stage
+// k+1, which reads each x-line once to filter it and differentiate the
+// filtered line.  The state in HBM between two stages therefore lacks its x
+// filter ("pending"); it is applied before anything outside the stage looks
+// at the state (the end of a run, a CFL time step, a host read).
+//
+//   x pass:  per field, F_x (if pending) -> write state -> d/dx, d2/dx2
+//            (xfused.cu); then d/dx of Ey, Ez with E computed from the state.
+//   y pass:  d/dy, d2/dy2, E, calcRHS, rkExecute, F_y.
+#include <cstring>
+
 #include "common.cuh"
+#include "xcore.cuh"
 
 namespace mhd {
-int fused_setup(Ctx *c) { (void)c; return MHDGPU_OK; }
-void fused_free(Ctx *c) { (void)c; }
+
+int fused_setup(Ctx *c) { return xfused_setup(c); }
+void fused_free(Ctx *c) { xfused_free(c); }
+
+static double planeb(const Ctx *c) { return (double)c->nx * c->ny * 8.0; }
+
+// x pass of a stage
+static int fused_x_pass(Ctx *c)
+{
+    const mhdgpu_params &p = c->p;
+    XFArgs a;
+    std::memset(&a, 0, sizeof a);
+    a.in = c->arr[MHDGPU_UU];
+    a.in_start = 0;
+    a.src_kind = 0;
+    a.fout = c->fused_pending_filter ? c->arr[MHDGPU_UU] : nullptr;
+    a.out1 = c->arr[MHDGPU_DUDX];
+    a.out2a = p.viscosity > 0 ? c->arr[MHDGPU_D2UDX2] : nullptr;
+    a.d2a_lo = UX;
+    a.out2b = (p.resistivity > 0 || p.Hall == 1) ? c->arr[MHDGPU_D2BDX2] : nullptr;
+    a.d2b_lo = BX;
+    a.single_op = -1;
+    int n2 = (a.out2a ? 3 : 0) + (a.out2b ? 3 : 0);
+    double bytes = planeb(c) * (c->nvar + (a.fout ? c->nvar : 0) + c->nvar + n2);
+    int rc = launch_xfused(c, a, c->nvar, bytes);
+    if (rc) return rc;
+    // d/dx of Ey, Ez (E from the filtered state) into dEdx[1], dEdx[2]
+    XFArgs e;
+    std::memset(&e, 0, sizeof e);
+    e.in = c->arr[MHDGPU_UU];
+    e.src_kind = 3;
+    e.single_op = XOP_D1;
+    e.out1 = c->arr[MHDGPU_DEDX] + (size_t)c->nx * c->ny;
+    return launch_xfused(c, e, 2, planeb(c) * (6 + 2));
+}
+
+// y pass of a stage
+static int fused_y_pass(Ctx *c, int iRK)
+{
+    const mhdgpu_params &p = c->p;
+    double *uu = c->arr[MHDGPU_UU];
+    int rc;
+    if ((rc = launch_yspec(c, 0, c->nvar, uu, 0, c->arr[MHDGPU_DUDY], 0))) return rc;
+    if (p.viscosity > 0 && (rc = launch_yspec(c, 1, 3, uu, UX, c->arr[MHDGPU_D2UDY2], 0))) return rc;
+    if ((p.resistivity > 0 || p.Hall == 1) &&
+        (rc = launch_yspec(c, 1, 3, uu, BX, c->arr[MHDGPU_D2BDY2], 0)))
+        return rc;
+    if ((rc = launch_efield(c))) return rc;
+    if ((rc = launch_yspec(c, 0, 3, c->arr[MHDGPU_EFIELD], 0, c->arr[MHDGPU_DEDY], 0))) return rc;
+    if ((rc = launch_rhs(c))) return rc;
+    if ((rc = launch_rk(c, iRK))) return rc;
+    return launch_yspec(c, 2, c->nvar, uu, 0, uu, 0);
+}
+
+int fused_apply_pending_filter(Ctx *c)
+{
+    if (!c->fused_pending_filter) return MHDGPU_OK;
+    XFArgs f;
+    std::memset(&f, 0, sizeof f);
+    f.in = c->arr[MHDGPU_UU];
+    f.single_op = XOP_F;
+    f.out1 = c->arr[MHDGPU_UU];
+    int rc = launch_xfused(c, f, c->nvar, planeb(c) * 2 * c->nvar);
+    if (rc) return rc;
+    c->fused_pending_filter = 0;
+    return MHDGPU_OK;
+}
+
 int fused_stage(Ctx *c, int iRK, int first, int last)
 {
-    (void)c; (void)iRK; (void)first; (void)last;
-    return mhd_set_error(MHDGPU_ERR_UNSUPPORTED);
+    (void)first;
+    (void)last;
+    int rc = fused_x_pass(c);
+    if (rc) return rc;
+    rc = fused_y_pass(c, iRK);
+    if (rc) return rc;
+    c->fused_pending_filter = 1;
+    return MHDGPU_OK;
 }
-}  // namespace mhd
 
-extern "C" int mhdgpu_steps_fused(mhdgpu_ctx *h, int nsteps, double dt_fixed, double *dt_io)
-{
-    (void)h; (void)nsteps; (void)dt_fixed; (void)dt_io;
-    return mhd_set_error(MHDGPU_ERR_UNSUPPORTED);
-}
+}  // namespace mhd

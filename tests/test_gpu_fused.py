@@ -1,0 +1,85 @@
+"""GPU: the fused two-pass stage (mhdgpu_steps_fused) against the reference
+and against the operator path, at the same gates as the operator path:
+1e-12 per field after one RK3 step, 1e-9 after 100 steps.
+"""
+import numpy as np
+import pytest
+
+import mhd_oracle as O
+from conftest import rel_l2
+from mhd2dcfdfftw_open_b200 import ic
+from mhd2dcfdfftw_open_b200.solver import Domain
+
+pytestmark = pytest.mark.gpu
+
+
+def run_ref(reference, p, uu, nsteps, dt_fixed):
+    reference.setup(p)
+    reference.set_state(uu)
+    _, dt = reference.steps(nsteps, dt_fixed)
+    return reference.uu.copy(), dt
+
+
+@pytest.mark.parametrize("nx,ny", [(64, 64), (96, 32), (40, 16)])
+def test_fused_1_step_vs_reference(reference, nx, ny):
+    p, uu = ic.orszag_tang(nx, ny, di=0.05)
+    ru, _ = run_ref(reference, p, uu, 1, 1e-3)
+    with Domain(p, uu) as d:
+        d.steps(1, 1e-3, fused=True)
+        err = rel_l2(d.get("uu"), ru)
+    assert err.max() < 1e-12, err
+
+
+def test_fused_multi_step_vs_reference(reference):
+    p, uu = ic.orszag_tang(128, 64, di=0.05)
+    ru, _ = run_ref(reference, p, uu, 7, 1e-3)
+    with Domain(p, uu) as d:
+        d.steps(3, 1e-3, fused=True)   # two calls: the pending x filter is
+        d.steps(4, 1e-3, fused=True)   # settled at the end of each call
+        err = rel_l2(d.get("uu"), ru)
+    assert err.max() < 1e-11, err
+
+
+def test_fused_256_100_steps_vs_reference(reference):
+    p, uu = ic.orszag_tang(256, 256, di=0.05)
+    ru, _ = run_ref(reference, p, uu, 100, 1e-3)
+    with Domain(p, uu) as d:
+        d.steps(100, 1e-3, fused=True)
+        gu = d.get("uu")
+    err = rel_l2(gu, ru)
+    assert err.max() < 1e-9, err
+    assert O.energy(p, gu) == pytest.approx(O.energy(p, ru), rel=1e-12)
+    assert O.cross_helicity(p, gu) == pytest.approx(O.cross_helicity(p, ru), rel=1e-12, abs=1e-14)
+
+
+@pytest.mark.parametrize("nx,ny", [(4096, 64), (8192, 32), (2048, 128), (1000, 64)])
+def test_fused_matches_operator_path_long_lines(nx, ny):
+    p, uu = ic.alfvenic_turbulence(nx, ny, mmax=8)
+    with Domain(p, uu) as d:
+        d.steps(1, 2e-4)
+        a = d.get("uu")
+        d.set("uu", uu)
+        d.steps(1, 2e-4, fused=True)
+        b = d.get("uu")
+    assert rel_l2(b, a).max() < 1e-12
+
+
+def test_fused_cfl_and_hyperbolic_cleaning_vs_reference(reference):
+    p, uu = ic.orszag_tang(64, 32, di=0.05, divBcleaning=2)
+    uu[8] = 1e-3 * np.random.default_rng(7).standard_normal(uu.shape[1:])
+    for dt_fixed in (1e-3, -1.0):
+        ru, rdt = run_ref(reference, p, uu, 3, dt_fixed)
+        with Domain(p, uu) as d:
+            dt = d.steps(3, dt_fixed, fused=True)
+            err = rel_l2(d.get("uu"), ru)
+        assert dt == pytest.approx(rdt, rel=1e-12)
+        assert err.max() < 1e-11, err
+
+
+def test_fused_diffusive_cleaning_routes_to_operator_stage(reference):
+    p, uu = ic.orszag_tang(64, 32, di=0.05, divBcleaning=1)
+    ru, _ = run_ref(reference, p, uu, 2, 1e-3)
+    with Domain(p, uu) as d:
+        d.steps(2, 1e-3, fused=True)
+        err = rel_l2(d.get("uu"), ru)
+    assert err.max() < 1e-11, err
