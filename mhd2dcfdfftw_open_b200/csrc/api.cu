@@ -434,13 +434,14 @@ extern "C" int mhdgpu_steps(mhdgpu_ctx *h, int nsteps, double dt_fixed, double *
 }
 
 // Steps through the fused stage (fused.cu).  Diffusive cleaning
-// (divBcleaning == 1) needs d/dx, d/dy of divB inside the stage and runs
-// through the operator stage instead.
+// (divBcleaning == 1) needs d/dx, d/dy of divB inside the stage, and grids the
+// fused x pass cannot tile (an odd nx with 8 columns), run through the
+// operator stage instead.
 extern "C" int mhdgpu_steps_fused(mhdgpu_ctx *h, int nsteps, double dt_fixed, double *dt_io)
 {
     CTX_OR_FAIL(h);
     if (nsteps < 0) return mhd_set_error(MHDGPU_ERR_INVALID);
-    if (c->p.divBcleaning == 1) return mhdgpu_steps(h, nsteps, dt_fixed, dt_io);
+    if (c->p.divBcleaning == 1 || c->xf_W == 0) return mhdgpu_steps(h, nsteps, dt_fixed, dt_io);
     const bool need_dt = dt_fixed <= 0 || c->p.divBcleaning == 2;
     double dt = dt_io ? *dt_io : 0.0;
     if (need_dt) TRY(settle(c));

@@ -4,6 +4,7 @@
 // error plumbing of the C ABI.
 #pragma once
 
+#include <cuda.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -90,6 +91,7 @@ struct Ctx {
     double *xf_edge;
     double xf_inner[2][3];
     int xf_W, xf_C, xf_R;
+    CUtensorMap xl_tmap_big, xl_tmap_unit;  // uu as [nvar*nx rows][ny] for the x pass
 };
 
 }  // namespace mhd
@@ -126,8 +128,8 @@ int launch_rk(Ctx *c, int iRK);
 int launch_calc_dt(Ctx *c, double dt0, double *dt_out);
 int launch_max_divb(Ctx *c, double *out);
 int launch_diagnostics(Ctx *c, double *energy, double *ch, int *finite);
-int xfused_setup(Ctx *c);
-void xfused_free(Ctx *c);
+int xline_setup(Ctx *c);
+void xline_free(Ctx *c);
 int fused_setup(Ctx *c);
 void fused_free(Ctx *c);
 int fused_stage(Ctx *c, int iRK, int first_stage_of_run, int last_stage);

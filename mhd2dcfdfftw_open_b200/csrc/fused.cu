@@ -19,12 +19,12 @@
 
 namespace mhd {
 
-int fused_setup(Ctx *c) { return xfused_setup(c); }
-void fused_free(Ctx *c) { xfused_free(c); }
+int fused_setup(Ctx *c) { return xline_setup(c); }
+void fused_free(Ctx *c) { xline_free(c); }
 
 static double planeb(const Ctx *c) { return (double)c->nx * c->ny * 8.0; }
 
-// x pass of a stage
+// x pass of a stage: one launch for all fields and the electric field
 static int fused_x_pass(Ctx *c)
 {
     const mhdgpu_params &p = c->p;
@@ -32,7 +32,7 @@ static int fused_x_pass(Ctx *c)
     std::memset(&a, 0, sizeof a);
     a.in = c->arr[MHDGPU_UU];
     a.in_start = 0;
-    a.src_kind = 0;
+    a.nfields = c->nvar;
     a.fout = c->fused_pending_filter ? c->arr[MHDGPU_UU] : nullptr;
     a.out1 = c->arr[MHDGPU_DUDX];
     a.out2a = p.viscosity > 0 ? c->arr[MHDGPU_D2UDX2] : nullptr;
@@ -40,18 +40,10 @@ static int fused_x_pass(Ctx *c)
     a.out2b = (p.resistivity > 0 || p.Hall == 1) ? c->arr[MHDGPU_D2BDX2] : nullptr;
     a.d2b_lo = BX;
     a.single_op = -1;
+    a.outE = c->arr[MHDGPU_DEDX] + (size_t)c->nx * c->ny;  // dEdx[1], dEdx[2]
     int n2 = (a.out2a ? 3 : 0) + (a.out2b ? 3 : 0);
-    double bytes = planeb(c) * (c->nvar + (a.fout ? c->nvar : 0) + c->nvar + n2);
-    int rc = launch_xfused(c, a, c->nvar, bytes);
-    if (rc) return rc;
-    // d/dx of Ey, Ez (E from the filtered state) into dEdx[1], dEdx[2]
-    XFArgs e;
-    std::memset(&e, 0, sizeof e);
-    e.in = c->arr[MHDGPU_UU];
-    e.src_kind = 3;
-    e.single_op = XOP_D1;
-    e.out1 = c->arr[MHDGPU_DEDX] + (size_t)c->nx * c->ny;
-    return launch_xfused(c, e, 2, planeb(c) * (6 + 2));
+    double bytes = planeb(c) * (c->nvar + (a.fout ? c->nvar : 0) + c->nvar + n2 + 2);
+    return launch_xline(c, a, bytes);
 }
 
 // y pass of a stage
@@ -75,12 +67,13 @@ static int fused_y_pass(Ctx *c, int iRK)
 int fused_apply_pending_filter(Ctx *c)
 {
     if (!c->fused_pending_filter) return MHDGPU_OK;
-    XFArgs f;
-    std::memset(&f, 0, sizeof f);
-    f.in = c->arr[MHDGPU_UU];
-    f.single_op = XOP_F;
-    f.out1 = c->arr[MHDGPU_UU];
-    int rc = launch_xfused(c, f, c->nvar, planeb(c) * 2 * c->nvar);
+    XFArgs a;
+    std::memset(&a, 0, sizeof a);
+    a.in = c->arr[MHDGPU_UU];
+    a.nfields = c->nvar;
+    a.single_op = XOP_F;
+    a.out1 = c->arr[MHDGPU_UU];
+    int rc = launch_xline(c, a, planeb(c) * 2 * c->nvar);
     if (rc) return rc;
     c->fused_pending_filter = 0;
     return MHDGPU_OK;

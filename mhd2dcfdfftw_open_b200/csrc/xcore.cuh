@@ -4,6 +4,8 @@
 // waits.
 #pragma once
 
+#include <cuda.h>
+
 #include "common.cuh"
 
 namespace mhd {
@@ -28,6 +30,8 @@ struct XFArgs {
     double *out2b;        // second-derivative output for fields [d2b_lo, d2b_lo+3)
     int d2a_lo, d2b_lo;
     int single_op;        // -1: the fused program; else one XOp into out1
+    int nfields;          // state fields [in_start, in_start + nfields)
+    double *outE;         // d/dx of Ey, Ez (2 fields), or null
     XStencil st[3];
     XFTables tb;
     long nx, ny;
@@ -80,6 +84,18 @@ __device__ __forceinline__ void bulk_g2s(void *dst, const void *src, unsigned by
         : "memory");
 }
 
+// 2-D tensor-map TMA load of box {x: column, y: row} into shared memory,
+// completion counted on an mbarrier (x must be a multiple of 2 for doubles)
+__device__ __forceinline__ void tma_load_2d(void *dst, const CUtensorMap *map, int x, int y,
+                                            uint64_t *bar)
+{
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes"
+        " [%0], [%1, {%2, %3}], [%4];" ::"r"(smem_u32(dst)),
+        "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(smem_u32(bar))
+        : "memory");
+}
+
 __device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, unsigned parity)
 {
     uint32_t ok;
@@ -112,6 +128,6 @@ __device__ __forceinline__ long wrap(long r, long n)
     return r < 0 ? r + n : r;
 }
 
-int launch_xfused(Ctx *c, const XFArgs &proto, int nf, double bytes);
+int launch_xline(Ctx *c, const XFArgs &proto, double bytes);
 
 }  // namespace mhd

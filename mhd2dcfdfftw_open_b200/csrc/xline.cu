@@ -1,0 +1,653 @@
+// x pass of the fused RK3 stage (see fused.cu): for every field of the state
+// and every x-line, the compact filter (filterCFD, mathlib.c:296-354) when it
+// is pending, then the first derivative (derivCFD1st, mathlib.c:33-86) and,
+// for the velocity and magnetic components, the second derivative
+// (derivCFD2nd, mathlib.c:163-218) of the filtered line; then d/dx of Ey and
+// Ez computed from the filtered state.  Every solve is the non-cyclic Thomas
+// solve of tridiagonalSolver (mathlib.c:8-30).
+//
+// Layout of the work.  A cluster of C CTAs owns W adjacent columns over the
+// whole line and walks all fields of that column tile:
+//   * field v+1 is staged into the second of two shared-memory tiles by the
+//     TMA engine (cp.async.bulk, one W*8-byte copy per row, mbarrier
+//     completion) while field v is solved;
+//   * 1024 threads per CTA: thread (column, sub-chunk) keeps its 8 rows of a
+//     recurrence in registers; the exact inflows of each sub-chunk come from
+//     a warp-shuffle scan of the sub-chunk (end value, product) pairs inside
+//     the CTA and of the CTA pairs across the cluster, read through
+//     distributed shared memory;
+//   * the filtered line replaces the tile's core rows and its three halo rows
+//     on each side are copied from the neighbouring CTAs' tiles, so the line
+//     is read from HBM once for all three operators.
+// Rows away from the two line ends use the constant interior Thomas factors
+// and a branch-free interior stencil; the few sub-chunks that touch the first
+// or last XF_EDGE rows use the tabulated factors and the closure stencils.
+#include <cooperative_groups.h>
+
+#include <cudaTypedefs.h>
+
+#include <cstdlib>
+#include <cstring>
+#include <vector>
+
+#include "common.cuh"
+#include "xcore.cuh"
+
+namespace cg = cooperative_groups;
+
+namespace mhd {
+
+constexpr int XL_T = 1024;
+constexpr int XL_S = 8;  // rows of a recurrence per thread
+// Halo rows kept on each side of a CTA's rows (the stencils use 3): with 4,
+// every TMA copy starts on an even tile row, which keeps the shared-memory
+// destination of a copy 128-byte aligned for 8-column (64-byte) rows.
+constexpr int XL_H = 4;
+
+template <int W>
+struct XLGeom {
+    static constexpr int NSUB = XL_T / W;
+    static constexpr int RCAP = NSUB * XL_S;  // rows per CTA at most
+    static constexpr int TROWS = RCAP + 2 * XL_H;
+};
+
+// aggregate arrays are stored column-major with one pad slot per column
+// (index col * (NSUB + 1) + sub) so a scan warp reads consecutive sub-chunks
+template <int W>
+__host__ __device__ constexpr int xl_aggn() { return W * (XLGeom<W>::NSUB + 1); }
+
+template <int W>
+__host__ __device__ constexpr size_t xl_smem_bytes()
+{
+    return sizeof(double) * (2 * (size_t)XLGeom<W>::TROWS * W + 2 * 3 * 2 * XF_EDGE +
+                             4 * (size_t)xl_aggn<W>() + 2 * 4 * W) + 2 * sizeof(uint64_t);
+}
+
+struct XLSmem {
+    double *tile[2];
+    double *tab;
+    double *aggE, *aggP;   // sub-chunk end value and product (zero inflow)
+    double *preE, *preP;   // composite of the preceding sub-chunks of the CTA
+    double *cta[2];        // [fwY, fwP, bwX, bwQ] x W, alternating between solves
+    uint64_t *bar;
+};
+
+template <int W>
+__device__ __forceinline__ XLSmem xl_carve(unsigned char *raw)
+{
+    XLSmem s;
+    double *p = reinterpret_cast<double *>(raw);
+    s.tile[0] = p; p += (size_t)XLGeom<W>::TROWS * W;
+    s.tile[1] = p; p += (size_t)XLGeom<W>::TROWS * W;
+    s.tab = p; p += 2 * 3 * 2 * XF_EDGE;
+    s.aggE = p; p += xl_aggn<W>();
+    s.aggP = p; p += xl_aggn<W>();
+    s.preE = p; p += xl_aggn<W>();
+    s.preP = p; p += xl_aggn<W>();
+    s.cta[0] = p; p += 4 * W;
+    s.cta[1] = p; p += 4 * W;
+    s.bar = reinterpret_cast<uint64_t *>(p);
+    return s;
+}
+
+// Scan of first-order linear recurrences over the sub-chunks of each column:
+// warp `col` (< W) combines the (end value, product) pairs of the NSUB
+// sub-chunks in order (reversed for the backward sweep), writes the CTA total
+// to cta[off..] and the composite of the preceding sub-chunks to preE/preP.
+// Composition: segment A then B gives (E_B + P_B E_A, P_A P_B).
+template <int W>
+__device__ __forceinline__ void xl_scan(const XLSmem &s, double *cta, int off, bool reverse)
+{
+    constexpr int NSUB = XLGeom<W>::NSUB;
+    constexpr int K = NSUB / 32;  // sub-chunks per lane
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (warp >= W) return;
+    const int base = warp * (NSUB + 1);
+    double E = 0.0, P = 1.0;
+#pragma unroll
+    for (int j = 0; j < K; j++) {
+        int q = lane * K + j;
+        int sidx = reverse ? NSUB - 1 - q : q;
+        double e = s.aggE[base + sidx], p = s.aggP[base + sidx];
+        E = e + p * E;
+        P = p * P;
+    }
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        double Eo = __shfl_up_sync(0xffffffffu, E, o), Po = __shfl_up_sync(0xffffffffu, P, o);
+        if (lane >= o) {
+            E = E + P * Eo;
+            P = P * Po;
+        }
+    }
+    double Ex = __shfl_up_sync(0xffffffffu, E, 1), Px = __shfl_up_sync(0xffffffffu, P, 1);
+    if (lane == 0) {
+        Ex = 0.0;
+        Px = 1.0;
+    }
+    if (lane == 31) {
+        cta[off * W + warp] = E;
+        cta[(off + 1) * W + warp] = P;
+    }
+#pragma unroll
+    for (int j = 0; j < K; j++) {
+        int q = lane * K + j;
+        int sidx = reverse ? NSUB - 1 - q : q;
+        s.preE[base + sidx] = Ex;
+        s.preP[base + sidx] = Px;
+        double e = s.aggE[base + sidx], p = s.aggP[base + sidx];
+        Ex = e + p * Ex;
+        Px = p * Px;
+    }
+}
+
+// interior right-hand side of operator OP (rows 1..n-2 of the line)
+template <int OP>
+__device__ __forceinline__ double xl_rhs(const XStencil &s, double w0, double w1, double w2,
+                                         double w3, double w4, double w5, double w6)
+{
+    if (OP == XOP_D1) return s.scale * (s.a * (w4 - w2) + s.b * (w5 - w1) + s.c * (w6 - w0));
+    if (OP == XOP_D2)
+        return s.scale * (s.a * (w4 - 2 * w3 + w2) + s.b * (w5 - 2 * w3 + w1) + s.c * (w6 - 2 * w3 + w0));
+    return s.a * w3 + s.b * (w4 + w2) + s.c * (w5 + w1) + s.d * (w6 + w0);
+}
+
+// Thomas factor `which` (0 m, 1 invB, 2 g) of matrix `mat` at row gr < n:
+// tabulated near the line ends, the interior constant elsewhere
+__device__ __forceinline__ double xl_tab(const double *tab, const XFTables &tb, int mat, int which,
+                                         long gr, long n)
+{
+    const double *t = tab + (mat * 3 + which) * 2 * XF_EDGE;
+    if (gr < XF_EDGE) return t[gr];
+    if (gr >= n - XF_EDGE) return t[XF_EDGE + (gr - (n - XF_EDGE))];
+    return tb.inner[mat][which];
+}
+
+// Exact split Thomas solve of operator OP over the core rows of tile t.
+// Results go to global memory (column pointer gout, row stride ny) and/or
+// back into the tile's core rows (tout).  `par` alternates between calls so
+// that consecutive solves exchange carries through different arrays; the
+// caller issues a cluster barrier before reading results of other CTAs.
+template <int W, int OP>
+__device__ void xl_solve(const XFArgs &a, const XLSmem &s, cg::cluster_group &cluster,
+                         const double *t, double *gout, double *tout, int Rc, long r0, int crank,
+                         int par)
+{
+    constexpr int NSUB = XLGeom<W>::NSUB;
+    constexpr int MAT = OP == XOP_F ? 1 : 0;
+    const int tid = threadIdx.x, lane = tid % W, sub = tid / W;
+    const int ai = lane * (NSUB + 1) + sub;  // this thread's aggregate slot
+    const long nx = a.nx, ny = a.ny;
+    const int la = sub * XL_S;
+    const bool edge = (r0 + la < XF_EDGE) || (r0 + la + XL_S > nx - XF_EDGE);
+    const double m_in = a.tb.inner[MAT][0], ib_in = a.tb.inner[MAT][1], g_in = a.tb.inner[MAT][2];
+    double *cta = s.cta[par];
+    double y[XL_S];
+
+    // ---- forward recurrence with zero inflow ------------------------------
+    double yv = 0.0, P = 1.0;
+    {
+        const double *tw = t + (XL_H - 3) * W + lane;  // tw[r * W] = input of local row r - 3
+        double w0 = tw[(la + 0) * W], w1 = tw[(la + 1) * W], w2 = tw[(la + 2) * W];
+        double w3 = tw[(la + 3) * W], w4 = tw[(la + 4) * W], w5 = tw[(la + 5) * W];
+        if (!edge) {  // interior rows: constant factors, branch-free stencil
+#pragma unroll
+            for (int k = 0; k < XL_S; k++) {
+                const int l = la + k;
+                double w6 = tw[(l + 6) * W];
+                double rhs = xl_rhs<OP>(a.st[OP], w0, w1, w2, w3, w4, w5, w6);
+                if (l < Rc) {
+                    yv = rhs - m_in * yv;
+                    P *= -m_in;
+                }
+                y[k] = yv;
+                w0 = w1; w1 = w2; w2 = w3; w3 = w4; w4 = w5; w5 = w6;
+            }
+        } else {      // near a line end: tabulated factors, closure rows
+#pragma unroll
+            for (int k = 0; k < XL_S; k++) {
+                const int l = la + k;
+                const long gr = r0 + l;
+                double w6 = tw[(l + 6) * W];
+                if (l < Rc) {
+                    double rhs = stencil(a.st[OP], w0, w1, w2, w3, w4, w5, w6, gr, nx);
+                    double m = xl_tab(s.tab, a.tb, MAT, 0, gr, nx);
+                    yv = rhs - m * yv;
+                    P *= -m;
+                }
+                y[k] = yv;
+                w0 = w1; w1 = w2; w2 = w3; w3 = w4; w4 = w5; w5 = w6;
+            }
+        }
+    }
+    s.aggE[ai] = yv;
+    s.aggP[ai] = P;
+    __syncthreads();
+    xl_scan<W>(s, cta, 0, false);
+    cluster.sync();
+
+    // ---- forward inflow and fix-up; backward recurrence with zero inflow --
+    double cin = 0.0;
+    for (int c2 = 0; c2 < crank; c2++) {
+        const double *rc = cluster.map_shared_rank(cta, c2);
+        cin = rc[lane] + rc[W + lane] * cin;
+    }
+    double d = s.preE[ai] + s.preP[ai] * cin;
+    double xv = 0.0, Q = 1.0;
+    if (!edge) {
+#pragma unroll
+        for (int k = 0; k < XL_S; k++) {
+            if (la + k < Rc) {
+                d *= -m_in;
+                y[k] += d;
+            }
+        }
+#pragma unroll
+        for (int k = XL_S - 1; k >= 0; k--) {
+            if (la + k < Rc) {
+                xv = y[k] * ib_in - g_in * xv;
+                Q *= -g_in;
+                y[k] = xv;
+            }
+        }
+    } else {
+#pragma unroll
+        for (int k = 0; k < XL_S; k++) {
+            const int l = la + k;
+            if (l < Rc) {
+                d *= -xl_tab(s.tab, a.tb, MAT, 0, r0 + l, nx);
+                y[k] += d;
+            }
+        }
+#pragma unroll
+        for (int k = XL_S - 1; k >= 0; k--) {
+            const int l = la + k;
+            if (l < Rc) {
+                double g = xl_tab(s.tab, a.tb, MAT, 2, r0 + l, nx);
+                xv = y[k] * xl_tab(s.tab, a.tb, MAT, 1, r0 + l, nx) - g * xv;
+                Q *= -g;
+                y[k] = xv;
+            }
+        }
+    }
+    __syncthreads();  // everyone has read preE/preP before the scan rewrites them
+    s.aggE[ai] = xv;
+    s.aggP[ai] = Q;
+    __syncthreads();
+    xl_scan<W>(s, cta, 2, true);
+    cluster.sync();
+
+    // ---- backward inflow, fix-up and results -------------------------------
+    double cb = 0.0;
+    for (int c2 = a.C - 1; c2 > crank; c2--) {
+        const double *rc = cluster.map_shared_rank(cta, c2);
+        cb = rc[2 * W + lane] + rc[3 * W + lane] * cb;
+    }
+    d = s.preE[ai] + s.preP[ai] * cb;
+#pragma unroll
+    for (int k = XL_S - 1; k >= 0; k--) {
+        const int l = la + k;
+        if (l < Rc) {
+            d *= edge ? -xl_tab(s.tab, a.tb, MAT, 2, r0 + l, nx) : -g_in;
+            double v = y[k] + d;
+            if (gout) gout[(r0 + l) * ny] = v;
+            if (tout) tout[(l + XL_H) * W + lane] = v;
+        }
+    }
+}
+
+constexpr int XL_BOX = 256;  // rows of the large tensor-map box
+
+// The rows of tile [0, Rc+2H) come from field rows r0-H .. r0+Rc+H-1 with
+// periodic wrap: at most three contiguous runs.  Each run is copied with
+// 256-row boxes (the last box ends exactly at the run's end and may overlap
+// the previous one) or, when shorter than 256 rows, with U-row boxes, U = 2
+// for 8-column tiles (a 128-byte copy) and 1 otherwise.
+struct XLRun {
+    int toff;  // first tile row
+    long g;    // first field row
+    int len;
+};
+
+__device__ __forceinline__ int xl_runs(long r0, int Rc, long nx, XLRun run[3])
+{
+    int n = 0, toff = 0, left = Rc + 2 * XL_H;
+    long g = r0 - XL_H;
+    while (left > 0 && n < 3) {
+        long gw = g < 0 ? g + nx : (g >= nx ? g - nx : g);
+        int len = (int)min((long)left, nx - gw);
+        run[n++] = XLRun{toff, gw, len};
+        toff += len;
+        g += len;
+        left -= len;
+    }
+    return n;
+}
+
+// Issue the TMA copies of field `v` into tile buffer `b`; warp 0 only.
+template <int W>
+__device__ __forceinline__ void xl_stage(const XFArgs &a, const XLSmem &s, int b, int v, long r0,
+                                         int Rc, long j0, const CUtensorMap *big,
+                                         const CUtensorMap *unit)
+{
+    XLRun run[3];
+    const int nrun = xl_runs(r0, Rc, a.nx, run);
+    unsigned bytes = 0;
+    constexpr int U = W == 8 ? 2 : 1;
+    for (int q = 0; q < nrun; q++) {
+        int len = run[q].len;
+        int nbox = len >= XL_BOX ? (len + XL_BOX - 1) / XL_BOX : len / U;
+        bytes += (unsigned)nbox * (len >= XL_BOX ? XL_BOX : U) * W * 8u;
+    }
+    if (threadIdx.x == 0) {
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        mbar_expect_tx(&s.bar[b], bytes);
+    }
+    __syncwarp();
+    const long frow = (long)v * a.nx;
+    int k = 0;  // copy counter across runs, dealt round-robin to the lanes
+    for (int q = 0; q < nrun; q++) {
+        const int len = run[q].len;
+        if (len >= XL_BOX) {
+            const int nbox = (len + XL_BOX - 1) / XL_BOX;
+            for (int i = 0; i < nbox; i++, k++) {
+                if ((k & 31) != (int)threadIdx.x) continue;
+                int off = min(i * XL_BOX, len - XL_BOX);
+                double *dst = s.tile[b] + (size_t)(run[q].toff + off) * W;
+                if (smem_u32(dst) & 127u) {  // never issue a misaligned copy
+                    atomicExch(a.flag, MHDGPU_ERR_INVALID);
+                    continue;
+                }
+                tma_load_2d(dst, big, (int)j0, (int)(frow + run[q].g + off), &s.bar[b]);
+            }
+        } else {
+            for (int i = 0; i < len; i += U, k++) {
+                if ((k & 31) != (int)threadIdx.x) continue;
+                double *dst = s.tile[b] + (size_t)(run[q].toff + i) * W;
+                if (smem_u32(dst) & 127u) {  // never issue a misaligned copy
+                    atomicExch(a.flag, MHDGPU_ERR_INVALID);
+                    continue;
+                }
+                tma_load_2d(dst, unit, (int)j0, (int)(frow + run[q].g + i), &s.bar[b]);
+            }
+        }
+    }
+}
+
+template <int W>
+__global__ void __launch_bounds__(XL_T, 1)
+xline_kernel(XFArgs a, const __grid_constant__ CUtensorMap tm_big,
+             const __grid_constant__ CUtensorMap tm_unit)
+{
+    extern __shared__ __align__(128) unsigned char xl_raw[];
+    cg::cluster_group cluster = cg::this_cluster();
+    const int C = a.C;
+    const int crank = (int)cluster.block_rank();
+    const int tile = blockIdx.x / C;
+    const long nx = a.nx, ny = a.ny;
+    const long j0 = (long)tile * W;
+    const int ncols = (int)min((long)W, ny - j0);
+    const long r0 = (long)crank * a.R;
+    const int Rc = (int)min((long)a.R, nx - r0);
+    const size_t plane = (size_t)nx * ny;
+    const int tid = threadIdx.x, lane = tid % W;
+    const bool col = lane < ncols;
+    XLSmem s = xl_carve<W>(xl_raw);
+
+    for (int i = tid; i < 2 * 3 * 2 * XF_EDGE; i += XL_T) s.tab[i] = a.tb.edge[i];
+    if (tid == 0) {
+        mbar_init(&s.bar[0], 1);
+        mbar_init(&s.bar[1], 1);
+    }
+    __syncthreads();
+
+    const int nf = a.nfields;  // state fields [in_start, in_start + nf)
+    unsigned phase[2] = {0u, 0u};
+    int par = 0;  // alternates the carry-exchange arrays between solves
+    if (nf > 0 && tid < 32) xl_stage<W>(a, s, 0, a.in_start, r0, Rc, j0, &tm_big, &tm_unit);
+
+    for (int f = 0; f < nf; f++) {
+        const int b = f & 1;
+        const int v = a.in_start + f;
+        // the other tile is free: its last readers finished before the
+        // cluster barriers of the previous field's solves
+        if (f + 1 < nf && tid < 32) xl_stage<W>(a, s, b ^ 1, v + 1, r0, Rc, j0, &tm_big, &tm_unit);
+        mbar_wait_bounded(&s.bar[b], phase[b], a.flag);
+        phase[b] ^= 1u;
+        __syncthreads();
+        double *t = s.tile[b];
+        if (a.single_op >= 0) {  // one operator per field
+            double *g = (a.out1 && col) ? a.out1 + (size_t)f * plane + j0 + lane : nullptr;
+            if (a.single_op == XOP_F) xl_solve<W, XOP_F>(a, s, cluster, t, g, nullptr, Rc, r0, crank, par);
+            else if (a.single_op == XOP_D1) xl_solve<W, XOP_D1>(a, s, cluster, t, g, nullptr, Rc, r0, crank, par);
+            else xl_solve<W, XOP_D2>(a, s, cluster, t, g, nullptr, Rc, r0, crank, par);
+            par ^= 1;
+            continue;
+        }
+        if (a.fout) {
+            double *g = col ? a.fout + (size_t)v * plane + j0 + lane : nullptr;
+            xl_solve<W, XOP_F>(a, s, cluster, t, g, t, Rc, r0, crank, par);
+            par ^= 1;
+            cluster.sync();  // every CTA's tile holds its filtered core rows
+            // halo rows of the filtered line from the neighbouring CTAs
+            const int prv = (crank - 1 + C) % C, nxt = (crank + 1) % C;
+            const int Rp = (int)min((long)a.R, nx - (long)prv * a.R);
+            const double *tp = cluster.map_shared_rank(t, prv);
+            const double *tn = cluster.map_shared_rank(t, nxt);
+            if (tid < XL_H * W) {  // own halo rows: no other CTA reads them
+                int r = tid / W, cc = tid % W;
+                t[r * W + cc] = tp[(Rp + r) * W + cc];
+            } else if (tid < 2 * XL_H * W) {
+                int r = (tid - XL_H * W) / W, cc = tid % W;
+                t[(Rc + XL_H + r) * W + cc] = tn[(XL_H + r) * W + cc];
+            }
+            __syncthreads();
+        }
+        if (!a.out1) continue;
+        xl_solve<W, XOP_D1>(a, s, cluster, t, col ? a.out1 + (size_t)v * plane + j0 + lane : nullptr,
+                            nullptr, Rc, r0, crank, par);
+        par ^= 1;
+        double *g2 = nullptr;
+        if (a.out2a && v >= a.d2a_lo && v < a.d2a_lo + 3)
+            g2 = a.out2a + (size_t)(v - a.d2a_lo) * plane + j0 + lane;
+        else if (a.out2b && v >= a.d2b_lo && v < a.d2b_lo + 3)
+            g2 = a.out2b + (size_t)(v - a.d2b_lo) * plane + j0 + lane;
+        if (g2) {
+            xl_solve<W, XOP_D2>(a, s, cluster, t, col ? g2 : nullptr, nullptr, Rc, r0, crank, par);
+            par ^= 1;
+        }
+    }
+
+    if (a.outE) {
+        // d/dx of Ey = ux Bz - uz Bx and Ez = uy Bx - ux By from the
+        // (filtered) state this cluster has just written
+        __threadfence();
+        cluster.sync();
+        const double *u = a.in;
+        for (int e = 0; e < 2; e++) {
+            double *t = s.tile[e];
+            for (int idx = tid; idx < (Rc + 2 * XL_H) * W; idx += XL_T) {
+                int r = idx / W, c = idx % W;
+                if (c < ncols) {
+                    size_t o = (size_t)wrap(r0 - XL_H + r, nx) * ny + j0 + c;
+                    t[idx] = e == 0 ? u[UX * plane + o] * u[BZ * plane + o] - u[UZ * plane + o] * u[BX * plane + o]
+                                    : u[UY * plane + o] * u[BX * plane + o] - u[UX * plane + o] * u[BY * plane + o];
+                }
+            }
+            __syncthreads();
+            xl_solve<W, XOP_D1>(a, s, cluster, t, col ? a.outE + (size_t)e * plane + j0 + lane : nullptr,
+                                nullptr, Rc, r0, crank, par);
+            par ^= 1;
+        }
+    }
+    cluster.sync();  // peers may still read this CTA's shared memory
+}
+
+// ---------------------------------------------------------------------------
+// host side
+// ---------------------------------------------------------------------------
+
+// Thomas factors of the two matrices as xsolve.cu tabulates them: the first
+// and last XF_EDGE rows, and the interior constant, checked bit for bit.
+static int xline_tables(Ctx *c)
+{
+    const long n = c->nx;
+    std::vector<double> edge(2 * 3 * 2 * XF_EDGE, 0.0);
+    double inner[2][3];
+    for (int mat = 0; mat < 2; mat++) {
+        int op = mat == 0 ? XOP_D1 : XOP_F;
+        std::vector<double> h[3];
+        const double *dev[3] = {c->xt[op].m, c->xt[op].invB, c->xt[op].g};
+        for (int w = 0; w < 3; w++) {
+            h[w].resize(n);
+            MHD_CUDA_TRY(cudaMemcpy(h[w].data(), dev[w], sizeof(double) * n, cudaMemcpyDeviceToHost));
+        }
+        for (int w = 0; w < 3; w++) {
+            double *lo = edge.data() + (mat * 3 + w) * 2 * XF_EDGE;
+            double *hi = lo + XF_EDGE;
+            for (long i = 0; i < XF_EDGE; i++) {
+                lo[i] = i < n ? h[w][i] : 0.0;
+                long r = n - XF_EDGE + i;
+                hi[i] = r >= 0 ? h[w][r] : 0.0;
+            }
+            inner[mat][w] = n > 2 * XF_EDGE ? h[w][XF_EDGE] : 0.0;
+            for (long i = XF_EDGE; i < n - XF_EDGE; i++)
+                if (std::memcmp(&h[w][i], &inner[mat][w], sizeof(double)) != 0)
+                    return mhd_set_error(MHDGPU_ERR_UNSUPPORTED);  // interior not constant
+        }
+    }
+    MHD_CUDA_TRY(cudaMalloc(&c->xf_edge, sizeof(double) * edge.size()));
+    MHD_CUDA_TRY(cudaMemcpy(c->xf_edge, edge.data(), sizeof(double) * edge.size(),
+                            cudaMemcpyHostToDevice));
+    std::memcpy(c->xf_inner, inner, sizeof inner);
+    return MHDGPU_OK;
+}
+
+// Tensor map of a [rows][ny] double array with boxes of W columns x boxrows.
+static int xl_tensor_map(CUtensorMap *map, const double *base, long rows, long ny, int W,
+                         int boxrows)
+{
+    static PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
+    if (!encode) {
+        void *fn = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) !=
+                cudaSuccess ||
+            q != cudaDriverEntryPointSuccess || !fn)
+            return mhd_set_error(MHDGPU_ERR_CUDA);
+        encode = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
+    }
+    cuuint64_t gdim[2] = {(cuuint64_t)ny, (cuuint64_t)rows};
+    cuuint64_t gstride[1] = {(cuuint64_t)ny * sizeof(double)};
+    cuuint32_t box[2] = {(cuuint32_t)W, (cuuint32_t)boxrows};
+    cuuint32_t estride[2] = {1, 1};
+    CUresult r = encode(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 2, const_cast<double *>(base), gdim,
+                        gstride, box, estride, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                        CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                        CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    return r == CUDA_SUCCESS ? MHDGPU_OK : mhd_set_error(MHDGPU_ERR_UNSUPPORTED);
+}
+
+static long xl_rcap(int W)
+{
+    return W == 32 ? XLGeom<32>::RCAP : W == 16 ? XLGeom<16>::RCAP : XLGeom<8>::RCAP;
+}
+
+int xline_setup(Ctx *c)
+{
+    int rc = xline_tables(c);
+    if (rc) return rc;
+    const long n = c->nx;
+    // One CTA holds up to RCAP rows of W columns.  Short lines take W = 32 in
+    // one CTA; longer lines take W = 8 (1024 rows per CTA), which keeps the
+    // clusters small (4 CTAs for 4096 rows) so more of them fit on the GPU.
+    // MHDGPU_XLINE_W (8, 16 or 32) overrides the choice.
+    int W = n <= XLGeom<32>::RCAP ? 32 : 8;
+    if (const char *e = getenv("MHDGPU_XLINE_W")) {
+        int w = atoi(e);
+        if (w == 8 || w == 16 || w == 32) W = w;
+    }
+    while (W > 8 && W > c->ny) W /= 2;  // a tile never spans more columns than the grid
+    const long rcap = xl_rcap(W);
+    int C = (int)((n + rcap - 1) / rcap);
+    if (C > MHD_MAX_CLUSTER) return mhd_set_error(MHDGPU_ERR_UNSUPPORTED);
+    long R = (n + C - 1) / C;
+    if (W == 8 && (R % 2 || n % 2)) {  // 64-byte rows: copies must start on even rows
+        W = 16;
+        C = (int)((n + xl_rcap(W) - 1) / xl_rcap(W));
+        R = (n + C - 1) / C;
+    }
+    // Grids the fused x pass cannot tile run their steps through the operator
+    // stage instead (xf_W = 0; see mhdgpu_steps_fused).
+    if (W > c->ny || C > MHD_MAX_CLUSTER || R < XL_H || n - (long)(C - 1) * R < XL_H) {
+        c->xf_W = 0;
+        return MHDGPU_OK;
+    }
+    c->xf_W = W;
+    c->xf_C = C;
+    c->xf_R = (int)R;
+    const long rows = (long)c->nvar * n;
+    if ((rc = xl_tensor_map(&c->xl_tmap_big, c->arr[MHDGPU_UU], rows, c->ny, W, XL_BOX))) return rc;
+    if ((rc = xl_tensor_map(&c->xl_tmap_unit, c->arr[MHDGPU_UU], rows, c->ny, W, W == 8 ? 2 : 1)))
+        return rc;
+    MHD_CUDA_TRY(cudaFuncSetAttribute(xline_kernel<32>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)xl_smem_bytes<32>()));
+    MHD_CUDA_TRY(cudaFuncSetAttribute(xline_kernel<16>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)xl_smem_bytes<16>()));
+    MHD_CUDA_TRY(cudaFuncSetAttribute(xline_kernel<8>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)xl_smem_bytes<8>()));
+    if (C > 8) {
+        MHD_CUDA_TRY(cudaFuncSetAttribute(xline_kernel<32>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
+        MHD_CUDA_TRY(cudaFuncSetAttribute(xline_kernel<16>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
+        MHD_CUDA_TRY(cudaFuncSetAttribute(xline_kernel<8>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
+    }
+    return MHDGPU_OK;
+}
+
+void xline_free(Ctx *c)
+{
+    cudaFree(c->xf_edge);
+    c->xf_edge = nullptr;
+}
+
+int launch_xline(Ctx *c, const XFArgs &proto, double bytes)
+{
+    if (proto.nfields > 0 && proto.in != c->arr[MHDGPU_UU]) return mhd_set_error(MHDGPU_ERR_INVALID);
+    XFArgs a = proto;
+    for (int k = 0; k < 3; k++) a.st[k] = c->xs[k];
+    a.tb.edge = c->xf_edge;
+    std::memcpy(a.tb.inner, c->xf_inner, sizeof a.tb.inner);
+    a.nx = c->nx;
+    a.ny = c->ny;
+    a.R = c->xf_R;
+    a.C = c->xf_C;
+    a.flag = c->dflag;
+    const int W = c->xf_W;
+    const int ntiles = (int)((c->ny + W - 1) / W);
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(ntiles * a.C, 1, 1);
+    cfg.blockDim = dim3(XL_T, 1, 1);
+    cfg.stream = c->stream;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = a.C;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    prof_begin(c, KC_FUSED_X, bytes);
+    if (W == 32) {
+        cfg.dynamicSmemBytes = xl_smem_bytes<32>();
+        MHD_CUDA_TRY(cudaLaunchKernelEx(&cfg, xline_kernel<32>, a, c->xl_tmap_big, c->xl_tmap_unit));
+    } else if (W == 16) {
+        cfg.dynamicSmemBytes = xl_smem_bytes<16>();
+        MHD_CUDA_TRY(cudaLaunchKernelEx(&cfg, xline_kernel<16>, a, c->xl_tmap_big, c->xl_tmap_unit));
+    } else {
+        cfg.dynamicSmemBytes = xl_smem_bytes<8>();
+        MHD_CUDA_TRY(cudaLaunchKernelEx(&cfg, xline_kernel<8>, a, c->xl_tmap_big, c->xl_tmap_unit));
+    }
+    prof_end(c);
+    return MHDGPU_OK;
+}
+
+}  // namespace mhd
