@@ -79,13 +79,15 @@ int fused_apply_pending_filter(Ctx *c)
     return MHDGPU_OK;
 }
 
+bool yrow_supported(const Ctx *c);
+int launch_yrow(Ctx *c, int iRK, int last_stage);
+
 int fused_stage(Ctx *c, int iRK, int first, int last)
 {
     (void)first;
-    (void)last;
     int rc = fused_x_pass(c);
     if (rc) return rc;
-    rc = fused_y_pass(c, iRK);
+    rc = yrow_supported(c) ? launch_yrow(c, iRK, last) : fused_y_pass(c, iRK);
     if (rc) return rc;
     c->fused_pending_filter = 1;
     return MHDGPU_OK;

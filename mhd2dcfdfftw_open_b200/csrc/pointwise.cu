@@ -10,6 +10,7 @@
 
 #include "common.cuh"
 #include "dtcore.cuh"
+#include "rhscore.cuh"
 
 namespace mhd {
 
@@ -51,58 +52,38 @@ struct RhsArgs {
     int cleaning;
 };
 
-// calcRHSInnerPoint on the whole periodic domain, then addSourceTerm; the
-// expressions keep the reference's order of operations.
+// calcRHSInnerPoint on the whole periodic domain, then addSourceTerm
+// (rhs_point, rhscore.cuh)
 __global__ void rhs_kernel(RhsArgs a)
 {
     const long plane = a.plane;
+    RhsCoef k{a.gamma, a.visc, a.resist, a.cdiff, a.Ch, a.Cp, a.cleaning};
+    const int nv = a.cleaning == 2 ? 9 : 8;
     for (long o = blockIdx.x * (long)blockDim.x + threadIdx.x; o < plane;
          o += (long)gridDim.x * blockDim.x) {
-        const double *u = a.uu, *dx = a.dudx, *dy = a.dudy;
-#define F(arr, v) arr[(v) * plane + o]
-        double rho = F(u, RHO), ux = F(u, UX), uy = F(u, UY);
-        double bx = F(u, BX), by = F(u, BY), bz = F(u, BZ), pr = F(u, P);
-        double divU = F(dx, UX) + F(dy, UY);
-        double divB = F(dx, BX) + F(dy, BY);
-        double jx = F(dy, BZ);
-        double jy = -F(dx, BZ);
-        double jz = F(dx, BY) - F(dy, BX);
-        double r_rho = -rho * divU - ux * F(dx, RHO) - uy * F(dy, RHO);
-        double r_ux = -ux * F(dx, UX) - uy * F(dy, UX) - F(dx, P) / rho + jy * bz / rho - jz * by / rho;
-        double r_uy = -ux * F(dx, UY) - uy * F(dy, UY) - F(dy, P) / rho + jz * bx / rho - jx * bz / rho;
-        double r_uz = -ux * F(dx, UZ) - uy * F(dy, UZ) + jx * by / rho - jy * bx / rho;
-        double r_bx = -a.dEdy[2 * plane + o];
-        double r_by = a.dEdx[2 * plane + o];
-        double r_bz = a.dEdy[o] - a.dEdx[plane + o];
-        double r_p = -ux * F(dx, P) - uy * F(dy, P) - a.gamma * pr * divU;
-        double r_psi = 0.0;
-        if (a.cleaning == 2) {
-            r_ux = r_ux - divB * bx;
-            r_uy = r_uy - divB * by;
-            r_uz = r_uz - divB * bz;
-            r_bx = r_bx - F(dx, PSI);
-            r_by = r_by - F(dy, PSI);
-            r_psi = -a.Ch * a.Ch * (divB + F(u, PSI) / a.Cp / a.Cp);
+        double u[9], dx[9], dy[9], d2x[6], d2y[6], r[9];
+#pragma unroll
+        for (int v = 0; v < 9; v++) {
+            if (v < nv) {
+                u[v] = a.uu[v * plane + o];
+                dx[v] = a.dudx[v * plane + o];
+                dy[v] = a.dudy[v * plane + o];
+            } else {
+                u[v] = dx[v] = dy[v] = 0.0;
+            }
         }
-        if (a.visc > 0) {
-            r_ux = r_ux + a.visc / rho * (a.d2udx2[o] + a.d2udy2[o]);
-            r_uy = r_uy + a.visc / rho * (a.d2udx2[plane + o] + a.d2udy2[plane + o]);
-            r_uz = r_uz + a.visc / rho * (a.d2udx2[2 * plane + o] + a.d2udy2[2 * plane + o]);
+#pragma unroll
+        for (int c = 0; c < 3; c++) {
+            d2x[c] = a.visc > 0 ? a.d2udx2[c * plane + o] : 0.0;
+            d2y[c] = a.visc > 0 ? a.d2udy2[c * plane + o] : 0.0;
+            d2x[3 + c] = a.resist > 0 ? a.d2Bdx2[c * plane + o] : 0.0;
+            d2y[3 + c] = a.resist > 0 ? a.d2Bdy2[c * plane + o] : 0.0;
         }
-        if (a.resist > 0) {
-            r_bx = r_bx + a.resist * (a.d2Bdx2[o] + a.d2Bdy2[o]);
-            r_by = r_by + a.resist * (a.d2Bdx2[plane + o] + a.d2Bdy2[plane + o]);
-            r_bz = r_bz + a.resist * (a.d2Bdx2[2 * plane + o] + a.d2Bdy2[2 * plane + o]);
-        }
-        if (a.cleaning == 1) {
-            r_bx = r_bx + a.cdiff * a.ddivBdx[o];
-            r_by = r_by + a.cdiff * a.ddivBdy[o];
-        }
-        double *d = a.dudt;
-        F(d, RHO) = r_rho; F(d, UX) = r_ux; F(d, UY) = r_uy; F(d, UZ) = r_uz;
-        F(d, BX) = r_bx; F(d, BY) = r_by; F(d, BZ) = r_bz; F(d, P) = r_p;
-        if (a.cleaning == 2) F(d, PSI) = r_psi;
-#undef F
+        double dbx = a.cleaning == 1 ? a.ddivBdx[o] : 0.0;
+        double dby = a.cleaning == 1 ? a.ddivBdy[o] : 0.0;
+        rhs_point(k, u, dx, dy, d2x, d2y, a.dEdx[plane + o], a.dEdx[2 * plane + o], a.dEdy[o],
+                  a.dEdy[2 * plane + o], dbx, dby, r);
+        for (int v = 0; v < nv; v++) a.dudt[v * plane + o] = r[v];
     }
 }
 
