@@ -73,5 +73,13 @@ def build(force: bool = False, verbose: bool = False) -> str:
     return LIB
 
 
+def build_dropin_demo(ref_dir: str = "/root/reference") -> None:
+    """Link the reference's own driver against the drop-in layer (needs the
+    reference sources; outputs go to oracle/_ref/)."""
+    build()
+    subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle"), f"REF_DIR={ref_dir}",
+                    "dropin"], check=True)
+
+
 if __name__ == "__main__":
     build(force="--force" in sys.argv, verbose=True)

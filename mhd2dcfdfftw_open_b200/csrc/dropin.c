@@ -1,0 +1,255 @@
+/*
+ * The reference's hot-path entry points on the GPU (include/mhd_gpu_dropin.h).
+ *
+ * The reference keeps its state in globals defined by its initialize.c
+ * (declared in its initialize.h:11-69, `real` = double); this file declares
+ * the ones it uses with the same names and types.  Each entry point uploads
+ * the global arrays it reads, runs the operator of libmhdgpu.so on them, and
+ * downloads the arrays it writes, so the host globals stay exactly what the
+ * reference's own routines would leave there.
+ */
+#include <math.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+
+#include "mhd_gpu.h"
+#include "mhd_gpu_dropin.h"
+
+/* --- the reference's globals (initialize.c:15-79, divBcleaning.c:4) ------ */
+extern int NVAR;
+extern int boundaryTypeX;
+extern double cfl, Tmax, dtOut;
+extern size_t nx, ny, iSize, jSize;
+extern double Lx, Ly;
+extern double adiabaticIdx, resistivity, viscosity;
+extern int Hall, divBcleaning, outDivB;
+extern double di;
+extern double Ch_divBcleaning, Cp_divBcleaning;
+extern double Cr_divBCleaning;
+extern double *uu, *dudx, *dudy, *d2udx2, *d2udy2, *d2Bdx2, *d2Bdy2;
+extern double *divB, *ddivBdx, *ddivBdy, *Efield, *dEdx, *dEdy, *dudt, *dudtRK;
+extern double *uuHaloX0, *uuHaloX1, *divBHaloX0, *divBHaloX1, *EfieldHaloX0, *EfieldHaloX1;
+
+static mhdgpu_ctx *g_ctx = NULL;
+static size_t g_nx = 0, g_ny = 0;
+static int g_reported = 0;
+
+static void report(const char *where, int rc)
+{
+    if (rc != MHDGPU_OK && !g_reported) {
+        fprintf(stderr, "mhdgpu drop-in: %s failed: %s\n", where, mhdgpu_error_string(rc));
+        g_reported = 1;
+    }
+}
+
+/* the context, created from the globals initialize() has set */
+static mhdgpu_ctx *ctx(void)
+{
+    if (g_ctx && g_nx == nx && g_ny == ny) return g_ctx;
+    if (g_ctx) mhdgpu_destroy(g_ctx);
+    mhdgpu_params p;
+    p.boundaryTypeX = boundaryTypeX;
+    p.cfl = cfl;
+    p.Tmax = Tmax;
+    p.dtOut = dtOut;
+    p.nx = (long)nx;
+    p.ny = (long)ny;
+    p.Lx = Lx;
+    p.Ly = Ly;
+    p.adiabaticIdx = adiabaticIdx;
+    p.Hall = Hall;
+    p.di = di;
+    p.resistivity = resistivity;
+    p.viscosity = viscosity;
+    p.divBcleaning = divBcleaning;
+    p.outDivB = outDivB;
+    const char *dev = getenv("MHDGPU_DEVICE");
+    int rc = mhdgpu_create(&p, dev ? atoi(dev) : 0, &g_ctx);
+    if (rc != MHDGPU_OK) {
+        report("context creation", rc);
+        g_ctx = NULL;
+        return NULL;
+    }
+    g_nx = nx;
+    g_ny = ny;
+    return g_ctx;
+}
+
+/* the context array mirroring a reference global, or -1 */
+static int which(const double *a)
+{
+    const double *g[MHDGPU_NARRAYS] = {uu, dudx, dudy, d2udx2, d2udy2, d2Bdx2, d2Bdy2, divB,
+                                       ddivBdx, ddivBdy, Efield, dEdx, dEdy, dudt, dudtRK};
+    if (!a) return -1;
+    for (int k = 0; k < MHDGPU_NARRAYS; k++)
+        if (g[k] == a) return k;
+    return -1;
+}
+
+static double *host_of(int k)
+{
+    double *g[MHDGPU_NARRAYS] = {uu, dudx, dudy, d2udx2, d2udy2, d2Bdx2, d2Bdy2, divB,
+                                 ddivBdx, ddivBdy, Efield, dEdx, dEdy, dudt, dudtRK};
+    return g[k];
+}
+
+static int up(mhdgpu_ctx *c, int k)
+{
+    double *h = host_of(k);
+    if (!h || !mhdgpu_device_array(c, k)) return MHDGPU_OK;  /* not allocated: not used */
+    return mhdgpu_set_array(c, k, h);
+}
+
+static int down(mhdgpu_ctx *c, int k)
+{
+    double *h = host_of(k);
+    if (!h || !mhdgpu_device_array(c, k)) return MHDGPU_OK;
+    return mhdgpu_get_array(c, k, h);
+}
+
+static void deriv(const char *name, int dir, int order, int nv, double *in, int start,
+                  double *out)
+{
+    mhdgpu_ctx *c = ctx();
+    if (!c) return;
+    int ki = which(in), ko = which(out);
+    if (ki < 0 || ko < 0) {
+        report(name, MHDGPU_ERR_INVALID);
+        return;
+    }
+    int rc = up(c, ki);
+    if (!rc) rc = dir == 0 ? mhdgpu_deriv_x(c, nv, ki, start, ko, order)
+                           : mhdgpu_deriv_y(c, nv, ki, start, ko, order);
+    if (!rc) rc = down(c, ko);
+    report(name, rc);
+}
+
+void derivX(int nv, double *arrMain, double *arrHalo0, double *arrHalo1, double *arrDeriv,
+            int iVarStartMain, int iVarStartHalo)
+{
+    (void)arrHalo0; (void)arrHalo1; (void)iVarStartHalo;  /* periodic wrap is in the kernel */
+    deriv("derivX", 0, 1, nv, arrMain, iVarStartMain, arrDeriv);
+}
+
+void derivXX(int nv, double *arrMain, double *arrHalo0, double *arrHalo1, double *arrDeriv,
+             int iVarStartMain, int iVarStartHalo)
+{
+    (void)arrHalo0; (void)arrHalo1; (void)iVarStartHalo;
+    deriv("derivXX", 0, 2, nv, arrMain, iVarStartMain, arrDeriv);
+}
+
+void derivY(int nv, double *arrMain, double *arrDeriv, int iVarStartMain)
+{
+    deriv("derivY", 1, 1, nv, arrMain, iVarStartMain, arrDeriv);
+}
+
+void derivYY(int nv, double *arrMain, double *arrDeriv, int iVarStartMain)
+{
+    deriv("derivYY", 1, 2, nv, arrMain, iVarStartMain, arrDeriv);
+}
+
+void calcEfield(void)
+{
+    mhdgpu_ctx *c = ctx();
+    if (!c) return;
+    int rc = up(c, MHDGPU_UU);
+    if (!rc) rc = mhdgpu_calc_efield(c);
+    if (!rc) rc = down(c, MHDGPU_EFIELD);
+    report("calcEfield", rc);
+}
+
+void calcDivB(void)
+{
+    mhdgpu_ctx *c = ctx();
+    if (!c) return;
+    int rc = up(c, MHDGPU_DUDX);
+    if (!rc) rc = up(c, MHDGPU_DUDY);
+    if (!rc) rc = mhdgpu_calc_divb(c);
+    if (!rc) rc = down(c, MHDGPU_DIVB);
+    report("calcDivB", rc);
+}
+
+void calcRHS(void)
+{
+    mhdgpu_ctx *c = ctx();
+    if (!c) return;
+    static const int reads[] = {MHDGPU_UU, MHDGPU_DUDX, MHDGPU_DUDY, MHDGPU_D2UDX2,
+                                MHDGPU_D2UDY2, MHDGPU_D2BDX2, MHDGPU_D2BDY2, MHDGPU_DDIVBDX,
+                                MHDGPU_DDIVBDY, MHDGPU_DEDX, MHDGPU_DEDY};
+    int rc = MHDGPU_OK;
+    for (size_t k = 0; k < sizeof reads / sizeof reads[0] && !rc; k++) rc = up(c, reads[k]);
+    if (!rc) rc = mhdgpu_calc_rhs(c);
+    if (!rc) rc = down(c, MHDGPU_DUDT);
+    report("calcRHS", rc);
+}
+
+void filtering(void)
+{
+    mhdgpu_ctx *c = ctx();
+    if (!c) return;
+    int rc = up(c, MHDGPU_UU);
+    if (!rc) rc = mhdgpu_filtering(c);
+    if (!rc) rc = down(c, MHDGPU_UU);
+    report("filtering", rc);
+}
+
+/* rkInit (timeAdvance.c:20-27): stage coefficients and dudtRK = 0, here and
+ * on the device */
+void rkInit(double dt)
+{
+    mhdgpu_ctx *c = ctx();
+    if (!c) return;
+    memset(dudtRK, 0, sizeof(double) * (size_t)NVAR * iSize * jSize);
+    report("rkInit", mhdgpu_rk_init(c, dt));
+}
+
+void rkExecute(int iRK)
+{
+    mhdgpu_ctx *c = ctx();
+    if (!c) return;
+    int rc = up(c, MHDGPU_UU);
+    if (!rc) rc = up(c, MHDGPU_DUDT);
+    if (!rc) rc = up(c, MHDGPU_DUDTRK);
+    if (!rc) rc = mhdgpu_rk_execute(c, iRK);
+    if (!rc) rc = down(c, MHDGPU_UU);
+    if (!rc) rc = down(c, MHDGPU_DUDTRK);
+    report("rkExecute", rc);
+}
+
+/* calcDt (timeAdvance.c:38-153); with hyperbolic cleaning it also sets the
+ * reference's Ch_divBcleaning / Cp_divBcleaning (divBcleaning.c:7-10) */
+double calcDt(double dt0)
+{
+    mhdgpu_ctx *c = ctx();
+    if (!c) return dt0;
+    double dt = dt0;
+    int rc = up(c, MHDGPU_UU);
+    if (!rc) rc = mhdgpu_calc_dt(c, dt0, &dt);
+    if (!rc && divBcleaning == 2) {
+        double ch = 0.0, cp = 0.0;
+        rc = mhdgpu_get_cleaning_speeds(c, &ch, &cp);
+        Ch_divBcleaning = ch;
+        Cp_divBcleaning = sqrt(Cr_divBCleaning * ch);
+    }
+    report("calcDt", rc);
+    return dt;
+}
+
+/* The single-rank periodic halo exchange of parallel.c:13-24: the left halo
+ * holds rows nx-2, nx-1 and the right halo rows 0, 1 of every field. */
+static void halo(const double *a, int nf, double *h0, double *h1)
+{
+    if (!a || !h0 || !h1) return;
+    const size_t n = iSize, m = jSize;
+    for (int v = 0; v < nf; v++)
+        for (int r = 0; r < 2; r++) {
+            memcpy(h0 + ((size_t)v * 2 + r) * m, a + ((size_t)v * n + (n - 2 + r)) * m,
+                   sizeof(double) * m);
+            memcpy(h1 + ((size_t)v * 2 + r) * m, a + ((size_t)v * n + r) * m, sizeof(double) * m);
+        }
+}
+
+void sendrecvHaloPointsX(void) { halo(uu, NVAR, uuHaloX0, uuHaloX1); }
+void sendrecvHaloPointsdivBX(void) { halo(divB, 1, divBHaloX0, divBHaloX1); }
+void sendrecvHaloPointsEfieldX(void) { halo(Efield, 3, EfieldHaloX0, EfieldHaloX1); }

@@ -37,8 +37,14 @@ namespace cg = cooperative_groups;
 
 namespace mhd {
 
-constexpr int XL_T = 1024;
-constexpr int XL_S = 8;  // rows of a recurrence per thread
+#ifndef MHD_XLINE_THREADS
+#define MHD_XLINE_THREADS 1024
+#endif
+#ifndef MHD_XLINE_ROWS
+#define MHD_XLINE_ROWS 8
+#endif
+constexpr int XL_T = MHD_XLINE_THREADS;  // threads per CTA
+constexpr int XL_S = MHD_XLINE_ROWS;     // rows of a recurrence per thread
 // Halo rows kept on each side of a CTA's rows (the stencils use 3): with 4,
 // every TMA copy starts on an even tile row, which keeps the shared-memory
 // destination of a copy 128-byte aligned for 8-column (64-byte) rows.
@@ -99,7 +105,10 @@ template <int W>
 __device__ __forceinline__ void xl_scan(const XLSmem &s, double *cta, int off, bool reverse)
 {
     constexpr int NSUB = XLGeom<W>::NSUB;
-    constexpr int K = NSUB / 32;  // sub-chunks per lane
+    // sub-chunks per lane; with fewer sub-chunks than lanes the idle lanes
+    // carry the identity pair (0, 1)
+    constexpr int K = NSUB >= 32 ? NSUB / 32 : 1;
+    static_assert(NSUB < 32 || NSUB % 32 == 0, "sub-chunks per column must fill whole warps");
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     if (warp >= W) return;
     const int base = warp * (NSUB + 1);
@@ -107,6 +116,7 @@ __device__ __forceinline__ void xl_scan(const XLSmem &s, double *cta, int off, b
 #pragma unroll
     for (int j = 0; j < K; j++) {
         int q = lane * K + j;
+        if (q >= NSUB) break;
         int sidx = reverse ? NSUB - 1 - q : q;
         double e = s.aggE[base + sidx], p = s.aggP[base + sidx];
         E = e + p * E;
@@ -132,6 +142,7 @@ __device__ __forceinline__ void xl_scan(const XLSmem &s, double *cta, int off, b
 #pragma unroll
     for (int j = 0; j < K; j++) {
         int q = lane * K + j;
+        if (q >= NSUB) break;
         int sidx = reverse ? NSUB - 1 - q : q;
         s.preE[base + sidx] = Ex;
         s.preP[base + sidx] = Px;

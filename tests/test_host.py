@@ -109,3 +109,16 @@ def test_library_exports_every_declared_symbol():
     assert len(declared) >= 25
     missing = [n for n in declared if not hasattr(lib, n)]
     assert not missing, missing
+
+
+def test_dropin_archive_defines_the_reference_entry_points():
+    import subprocess
+    arc = os.path.join(ROOT, "mhd2dcfdfftw_open_b200", "libmhdgpu_dropin.a")
+    if not os.path.exists(arc):
+        pytest.skip("libmhdgpu_dropin.a not built")
+    text = re.sub(r"/\*.*?\*/", "", open(os.path.join(ROOT, "include", "mhd_gpu_dropin.h")).read(),
+                  flags=re.S)
+    declared = set(re.findall(r"\b(\w+)\s*\([^;{]*\)\s*;", text))
+    out = subprocess.run(["nm", arc], capture_output=True, text=True, check=True).stdout
+    defined = {ln.split()[-1] for ln in out.splitlines() if " T " in ln}
+    assert declared and declared <= defined, declared - defined
