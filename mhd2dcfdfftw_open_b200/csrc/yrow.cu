@@ -11,8 +11,9 @@
 //      fields.
 // The derivative rows pass through the context's dudy/d2udy2/d2Bdy2/dEdy
 // arrays, written in step 1 and read back in step 2 by the same CTA, so they
-// are served from L2; the updated state is written once by step 2 and the
-// filtered state once by step 3.
+// are served from L2; the updated state is written by step 2 and read back
+// (again from L2) and overwritten by step 3.  One padded FFT row per CTA row
+// and at most 128 registers per thread keep two CTAs on each SM.
 #include "common.cuh"
 #include "fft.cuh"
 #include "rhscore.cuh"
@@ -42,136 +43,100 @@ struct YRGeom {
     static constexpr int T = N / 16;                                  // threads per row
     static constexpr int ROWS = T >= YR_THREADS ? 1 : YR_THREADS / T;  // rows per CTA
     static constexpr int NP = N + N / 16;                             // padded row
-    // shared memory: FFT rows (ROWS x NP double2), staging of two raw rows
-    // per row (ROWS x 2N double), one mbarrier
-    static constexpr size_t SMEM = sizeof(double2) * ROWS * NP + sizeof(double) * ROWS * 2 * N + 16;
+    // shared memory: one padded FFT row per row of the CTA (68 KB for any
+    // row length), so that two CTAs share an SM
+    static constexpr size_t SMEM = sizeof(double2) * ROWS * NP;
 };
 
-// TMA bulk copies of state fields fa and fb (fb < 0: none) of the block's rows
-// into the staging buffer; called by warp 0.  Completion is counted on `bar`.
+// Load fields fa and fb (fb < 0: zero) of this group's row into the FFT row
+// as fa + i fb; each thread its own 16 points, coalesced across the group.
 template <int L>
-__device__ __forceinline__ void yr_prefetch(const YRArgs &a, double *S, uint64_t *bar, long row0,
-                                            int fa, int fb)
+__device__ __forceinline__ void yr_load(double2 *A, const double *ra, const double *rb, int j,
+                                        bool valid)
 {
     using G = YRGeom<L>;
-    const size_t plane = (size_t)a.nx * a.ny;
-    const int nrows = (int)min((long)G::ROWS, a.nx - row0);
-    const unsigned rowb = (unsigned)G::N * 8u;
-    if (threadIdx.x == 0) {
-        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-        mbar_expect_tx(bar, rowb * (unsigned)nrows * (fb >= 0 ? 2u : 1u));
-    }
-    __syncwarp();
-    for (int q = threadIdx.x; q < 2 * nrows; q += 32) {
-        const int g = q >> 1, which = q & 1;
-        const int fld = which ? fb : fa;
-        if (fld < 0) continue;
-        bulk_g2s(S + (size_t)g * 2 * G::N + (size_t)which * G::N,
-                 a.uu + (size_t)fld * plane + (size_t)(row0 + g) * a.ny, rowb, bar);
-    }
-}
-
-// Spectral operators of one pair: A holds the row packed as re + i im.
-// Forward FFT, then for each of up to two symbols: multiply, inverse FFT,
-// write the real part to oa and the imaginary part to ob (null: skipped).
-// The spectrum is kept in registers between the two operators.
-template <int L>
-__device__ void yr_ops(const YRArgs &a, double2 *A, int j, bool valid, long row,
-                       const double2 *sA, double *oA1, double *oB1, const double2 *sB, double *oA2,
-                       double *oB2)
-{
-    using G = YRGeom<L>;
-    const size_t ro = (size_t)row * a.ny;
-    fft_row<L, -1>(A, a.tw, j);
-    double2 Z[16];
-#pragma unroll
-    for (int m = 0; m < 16; m++) Z[m] = A[fpad(j + m * G::T)];
-    for (int op = 0; op < 2; op++) {
-        const double2 *s = op == 0 ? sA : sB;
-        double *oa = op == 0 ? oA1 : oA2, *ob = op == 0 ? oB1 : oB2;
-        if (!s) continue;  // uniform across the block
-        if (op == 1) __syncthreads();  // previous inverse FFT's results are stored
-#pragma unroll
-        for (int m = 0; m < 16; m++) {
-            const int i = j + m * G::T;
-            A[fpad(i)] = cm(Z[m], __ldg(s + i));
-        }
-        __syncthreads();
-        fft_row<L, +1>(A, a.tw, j);
-        if (valid) {
-#pragma unroll
-            for (int m = 0; m < 16; m++) {
-                const int i = j + m * G::T;
-                double2 z = A[fpad(i)];
-                if (oa) oa[ro + i] = z.x;
-                if (ob) ob[ro + i] = z.y;
-            }
-        }
-    }
-    __syncthreads();
-}
-
-// Unpack the staged raw rows of this group into the FFT row.
-template <int L>
-__device__ __forceinline__ void yr_unpack(double2 *A, const double *Sg, int j, bool two)
-{
-    using G = YRGeom<L>;
+    double va[16], vb[16];
 #pragma unroll
     for (int m = 0; m < 16; m++) {
         const int i = j + m * G::T;
-        A[fpad(i)] = make_double2(Sg[i], two ? Sg[G::N + i] : 0.0);
+        va[m] = valid ? ra[i] : 0.0;
+        vb[m] = (valid && rb) ? rb[i] : 0.0;
     }
+#pragma unroll
+    for (int m = 0; m < 16; m++) A[fpad(j + m * G::T)] = make_double2(va[m], vb[m]);
+}
+
+// One spectral operator on the row in A (natural order, already loaded):
+// forward FFT, multiply by the symbol s, inverse FFT, real part to oa and
+// imaginary part to ob (null: skipped).  Ends with the block synchronised.
+template <int L>
+__device__ __forceinline__ void yr_op(const YRArgs &a, double2 *A, int j, bool valid,
+                                      const double2 *s, double *oa, double *ob)
+{
+    using G = YRGeom<L>;
+    __syncthreads();  // the row is complete
+    fft_row<L, -1>(A, a.tw, j);
+#pragma unroll
+    for (int m = 0; m < 16; m++) {
+        const int i = j + m * G::T;
+        A[fpad(i)] = cm(A[fpad(i)], __ldg(s + i));
+    }
+    __syncthreads();
+    fft_row<L, +1>(A, a.tw, j);
+    if (valid) {
+#pragma unroll
+        for (int m = 0; m < 16; m++) {
+            const int i = j + m * G::T;
+            double2 z = A[fpad(i)];
+            if (oa) oa[i] = z.x;
+            if (ob) ob[i] = z.y;
+        }
+    }
+    __syncthreads();  // A may be refilled
 }
 
 template <int L>
-__global__ void __launch_bounds__(YR_THREADS, 1) yrow_kernel(YRArgs a)
+__global__ void __launch_bounds__(YR_THREADS, 2) yrow_kernel(YRArgs a)
 {
     using G = YRGeom<L>;
     extern __shared__ __align__(128) unsigned char yr_raw[];
     double2 *Abase = reinterpret_cast<double2 *>(yr_raw);
-    double *S = reinterpret_cast<double *>(Abase + (size_t)G::ROWS * G::NP);
-    uint64_t *bar = reinterpret_cast<uint64_t *>(S + (size_t)G::ROWS * 2 * G::N);
     const int g = threadIdx.x / G::T, j = threadIdx.x % G::T;
-    const long row0 = (long)blockIdx.x * G::ROWS;
-    const long row = row0 + g;
+    const long row = (long)blockIdx.x * G::ROWS + g;
     const bool valid = row < a.nx;
     double2 *A = Abase + (size_t)g * G::NP;
-    const double *Sg = S + (size_t)g * 2 * G::N;
     const size_t plane = (size_t)a.nx * a.ny;
-    auto f = [&](double *base, int v) -> double * { return base ? base + (size_t)v * plane : nullptr; };
-    unsigned ph = 0;
+    const size_t ro = valid ? (size_t)row * a.ny : 0;
+    // row `ro` of field v of array base (null base: null)
+    auto f = [&](double *base, int v) -> double * {
+        return base ? base + (size_t)v * plane + ro : nullptr;
+    };
+    auto fc = [&](const double *base, int v) -> const double * {
+        return base ? base + (size_t)v * plane + ro : nullptr;
+    };
 
-    if (threadIdx.x == 0) mbar_init(bar, 1);
-    __syncthreads();
-
-    // ---- 1. y-derivatives; the pairs' rows are staged by TMA one pair ahead
-    // (pairs: (ux,uy) (rho,p) (uz,Bz) (Bx,By) [psi]; (Ex,Ez) is formed from
-    // the state with plain loads)
-    const int pa[5] = {UX, RHO, UZ, BX, PSI};
-    const int pb[5] = {UY, P, BZ, BY, -1};
+    // ---- 1. y-derivatives: pairs (ux,uy) (rho,p) (uz,Bz) (Bx,By) [psi],
+    // d/dy of every field, d2/dy2 of u and B (a second forward FFT of the
+    // pair, reloaded from L2, instead of keeping the spectrum)
     const int npair = a.nvar == 9 ? 5 : 4;
-    if (threadIdx.x < 32) yr_prefetch<L>(a, S, bar, row0, pa[0], pb[0]);
     for (int q = 0; q < npair; q++) {
-        mbar_wait_bounded(bar, ph, a.flag);
-        ph ^= 1u;
-        yr_unpack<L>(A, Sg, j, pb[q] >= 0);
-        __syncthreads();  // staging consumed: the next pair may land in it
-        if (q + 1 < npair && threadIdx.x < 32) yr_prefetch<L>(a, S, bar, row0, pa[q + 1], pb[q + 1]);
-        const int fa = pa[q], fb = pb[q];
-        const double2 *s2 = nullptr;
+        const int fa = q == 0 ? UX : q == 1 ? RHO : q == 2 ? UZ : q == 3 ? BX : PSI;
+        const int fb = q == 0 ? UY : q == 1 ? P : q == 2 ? BZ : q == 3 ? BY : -1;
+        yr_load<L>(A, fc(a.uu, fa), fb >= 0 ? fc(a.uu, fb) : nullptr, j, valid);
+        yr_op<L>(a, A, j, valid, a.s1, f(a.dudy, fa), fb >= 0 ? f(a.dudy, fb) : nullptr);
         double *o2a = nullptr, *o2b = nullptr;
-        if (fa == UX && a.d2u) { s2 = a.s2; o2a = f(a.d2udy2, 0); o2b = f(a.d2udy2, 1); }
-        if (fa == UZ && (a.d2u || a.d2b)) {
-            s2 = a.s2;
+        if (fa == UX && a.d2u) { o2a = f(a.d2udy2, 0); o2b = f(a.d2udy2, 1); }
+        if (fa == UZ) {
             o2a = a.d2u ? f(a.d2udy2, 2) : nullptr;
             o2b = a.d2b ? f(a.d2Bdy2, 2) : nullptr;
         }
-        if (fa == BX && a.d2b) { s2 = a.s2; o2a = f(a.d2Bdy2, 0); o2b = f(a.d2Bdy2, 1); }
-        yr_ops<L>(a, A, j, valid, row, a.s1, f(a.dudy, fa), fb >= 0 ? f(a.dudy, fb) : nullptr, s2,
-                  o2a, o2b);
+        if (fa == BX && a.d2b) { o2a = f(a.d2Bdy2, 0); o2b = f(a.d2Bdy2, 1); }
+        if (o2a || o2b) {  // uniform across the block
+            yr_load<L>(A, fc(a.uu, fa), fc(a.uu, fb), j, valid);
+            yr_op<L>(a, A, j, valid, a.s2, o2a, o2b);
+        }
     }
     {   // (Ex, Ez) = (uz By - uy Bz, uy Bx - ux By)
-        const size_t ro = (size_t)row * a.ny;
 #pragma unroll 4
         for (int m = 0; m < 16; m++) {
             const int i = j + m * G::T;
@@ -184,14 +149,13 @@ __global__ void __launch_bounds__(YR_THREADS, 1) yrow_kernel(YRArgs a)
             }
             A[fpad(i)] = z;
         }
-        __syncthreads();
-        yr_ops<L>(a, A, j, valid, row, a.s1, f(a.dEdy, 0), f(a.dEdy, 2), nullptr, nullptr, nullptr);
+        yr_op<L>(a, A, j, valid, a.s1, f(a.dEdy, 0), f(a.dEdy, 2));
     }
 
     // ---- 2. right-hand side and RK3 update, point by point ------------------
     if (valid) {
-        const size_t ro = (size_t)row * a.ny;
         const int nv = a.nvar;
+#pragma unroll 1
         for (int m = 0; m < 16; m++) {
             const size_t o = ro + j + m * G::T;
             double u[9], dx[9], dy[9], d2x[6], d2y[6], r[9];
@@ -224,25 +188,14 @@ __global__ void __launch_bounds__(YR_THREADS, 1) yrow_kernel(YRArgs a)
             }
         }
     }
-    // the updated rows are read back by the TMA (async proxy) below
-    asm volatile("fence.proxy.async.global;" ::: "memory");
-    __syncthreads();
+    __syncthreads();  // the updated rows are visible to the whole block
 
-    // ---- 3. spectral y filter of the updated fields, staged one pair ahead --
+    // ---- 3. spectral y filter of the updated fields, two at a time ----------
     const int nfp = (a.nvar + 1) / 2;
-    if (threadIdx.x < 32) yr_prefetch<L>(a, S, bar, row0, 0, 1);
     for (int q = 0; q < nfp; q++) {
         const int v = 2 * q, w = v + 1 < a.nvar ? v + 1 : -1;
-        mbar_wait_bounded(bar, ph, a.flag);
-        ph ^= 1u;
-        yr_unpack<L>(A, Sg, j, w >= 0);
-        __syncthreads();
-        if (q + 1 < nfp && threadIdx.x < 32) {
-            const int v2 = 2 * (q + 1), w2 = v2 + 1 < a.nvar ? v2 + 1 : -1;
-            yr_prefetch<L>(a, S, bar, row0, v2, w2);
-        }
-        yr_ops<L>(a, A, j, valid, row, a.sf, f(a.uu, v), w >= 0 ? f(a.uu, w) : nullptr, nullptr,
-                  nullptr, nullptr);
+        yr_load<L>(A, fc(a.uu, v), w >= 0 ? fc(a.uu, w) : nullptr, j, valid);
+        yr_op<L>(a, A, j, valid, a.sf, f(a.uu, v), w >= 0 ? f(a.uu, w) : nullptr);
     }
 }
 
