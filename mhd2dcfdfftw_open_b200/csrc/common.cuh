@@ -91,6 +91,8 @@ struct Ctx {
     double *xf_edge;
     double xf_inner[2][3];
     int xf_W, xf_C, xf_R;
+    int xf_hops;          // CTAs whose totals enter an inflow of the fused x pass
+    double xf_pw[2][2];   // interior sub-chunk products (-m)^S, (-g)^S per matrix
     CUtensorMap xl_tmap_big, xl_tmap_unit;  // uu as [nvar*nx rows][ny] for the x pass
 };
 

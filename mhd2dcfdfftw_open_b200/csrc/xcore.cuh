@@ -36,6 +36,8 @@ struct XFArgs {
     XFTables tb;
     long nx, ny;
     int R, C;
+    int hops;             // CTAs whose totals enter a CTA's inflow (C: all)
+    double pw[2][2];      // per matrix: (-m)^XL_S, (-g)^XL_S of the interior
     int *flag;
 };
 

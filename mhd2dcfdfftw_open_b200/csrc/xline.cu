@@ -26,6 +26,7 @@
 
 #include <cudaTypedefs.h>
 
+#include <cmath>
 #include <cstdlib>
 #include <cstring>
 #include <vector>
@@ -66,15 +67,18 @@ template <int W>
 __host__ __device__ constexpr size_t xl_smem_bytes()
 {
     return sizeof(double) * (2 * (size_t)XLGeom<W>::TROWS * W + 2 * 3 * 2 * XF_EDGE +
-                             4 * (size_t)xl_aggn<W>() + 2 * 4 * W) + 2 * sizeof(uint64_t);
+                             6 * (size_t)xl_aggn<W>() + 2 * 6 * W) + 2 * sizeof(uint64_t);
 }
 
+// Aggregates of the sub-chunk recurrences.  Up to two systems with the same
+// matrix are solved side by side, so they share the products P and carry
+// their own end values E[0], E[1].
 struct XLSmem {
     double *tile[2];
     double *tab;
-    double *aggE, *aggP;   // sub-chunk end value and product (zero inflow)
-    double *preE, *preP;   // composite of the preceding sub-chunks of the CTA
-    double *cta[2];        // [fwY, fwP, bwX, bwQ] x W, alternating between solves
+    double *aggE[2], *aggP;  // sub-chunk end values and product (zero inflow)
+    double *preE[2], *preP;  // composite of the preceding sub-chunks of the CTA
+    double *cta[2];          // [fwE0, fwE1, fwP, bwE0, bwE1, bwP] x W, alternating between solves
     uint64_t *bar;
 };
 
@@ -86,22 +90,24 @@ __device__ __forceinline__ XLSmem xl_carve(unsigned char *raw)
     s.tile[0] = p; p += (size_t)XLGeom<W>::TROWS * W;
     s.tile[1] = p; p += (size_t)XLGeom<W>::TROWS * W;
     s.tab = p; p += 2 * 3 * 2 * XF_EDGE;
-    s.aggE = p; p += xl_aggn<W>();
+    s.aggE[0] = p; p += xl_aggn<W>();
+    s.aggE[1] = p; p += xl_aggn<W>();
     s.aggP = p; p += xl_aggn<W>();
-    s.preE = p; p += xl_aggn<W>();
+    s.preE[0] = p; p += xl_aggn<W>();
+    s.preE[1] = p; p += xl_aggn<W>();
     s.preP = p; p += xl_aggn<W>();
-    s.cta[0] = p; p += 4 * W;
-    s.cta[1] = p; p += 4 * W;
+    s.cta[0] = p; p += 6 * W;
+    s.cta[1] = p; p += 6 * W;
     s.bar = reinterpret_cast<uint64_t *>(p);
     return s;
 }
 
 // Scan of first-order linear recurrences over the sub-chunks of each column:
-// warp `col` (< W) combines the (end value, product) pairs of the NSUB
-// sub-chunks in order (reversed for the backward sweep), writes the CTA total
-// to cta[off..] and the composite of the preceding sub-chunks to preE/preP.
+// warp `col` (< W) combines the (end values, product) of the NSUB sub-chunks
+// in order (reversed for the backward sweep), writes the CTA total to
+// cta[off * W ..] and the composite of the preceding sub-chunks to preE/preP.
 // Composition: segment A then B gives (E_B + P_B E_A, P_A P_B).
-template <int W>
+template <int W, int NR>
 __device__ __forceinline__ void xl_scan(const XLSmem &s, double *cta, int off, bool reverse)
 {
     constexpr int NSUB = XLGeom<W>::NSUB;
@@ -112,42 +118,56 @@ __device__ __forceinline__ void xl_scan(const XLSmem &s, double *cta, int off, b
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     if (warp >= W) return;
     const int base = warp * (NSUB + 1);
-    double E = 0.0, P = 1.0;
+    double E[NR], P = 1.0;
 #pragma unroll
-    for (int j = 0; j < K; j++) {
-        int q = lane * K + j;
+    for (int r = 0; r < NR; r++) E[r] = 0.0;
+#pragma unroll
+    for (int jq = 0; jq < K; jq++) {
+        int q = lane * K + jq;
         if (q >= NSUB) break;
         int sidx = reverse ? NSUB - 1 - q : q;
-        double e = s.aggE[base + sidx], p = s.aggP[base + sidx];
-        E = e + p * E;
+        const double p = s.aggP[base + sidx];
+#pragma unroll
+        for (int r = 0; r < NR; r++) E[r] = s.aggE[r][base + sidx] + p * E[r];
         P = p * P;
     }
+    // every lane takes part in every shuffle (full mask)
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) {
-        double Eo = __shfl_up_sync(0xffffffffu, E, o), Po = __shfl_up_sync(0xffffffffu, P, o);
+        double Eo[NR];
+#pragma unroll
+        for (int r = 0; r < NR; r++) Eo[r] = __shfl_up_sync(0xffffffffu, E[r], o);
+        const double Po = __shfl_up_sync(0xffffffffu, P, o);
         if (lane >= o) {
-            E = E + P * Eo;
+#pragma unroll
+            for (int r = 0; r < NR; r++) E[r] = E[r] + P * Eo[r];
             P = P * Po;
         }
     }
-    double Ex = __shfl_up_sync(0xffffffffu, E, 1), Px = __shfl_up_sync(0xffffffffu, P, 1);
-    if (lane == 0) {
-        Ex = 0.0;
-        Px = 1.0;
+    double Ex[NR];
+#pragma unroll
+    for (int r = 0; r < NR; r++) {
+        const double e = __shfl_up_sync(0xffffffffu, E[r], 1);
+        Ex[r] = lane == 0 ? 0.0 : e;
     }
+    const double pxs = __shfl_up_sync(0xffffffffu, P, 1);
+    double Px = lane == 0 ? 1.0 : pxs;
     if (lane == 31) {
-        cta[off * W + warp] = E;
-        cta[(off + 1) * W + warp] = P;
+#pragma unroll
+        for (int r = 0; r < NR; r++) cta[(off + r) * W + warp] = E[r];
+        cta[(off + 2) * W + warp] = P;
     }
 #pragma unroll
-    for (int j = 0; j < K; j++) {
-        int q = lane * K + j;
+    for (int jq = 0; jq < K; jq++) {
+        int q = lane * K + jq;
         if (q >= NSUB) break;
         int sidx = reverse ? NSUB - 1 - q : q;
-        s.preE[base + sidx] = Ex;
+#pragma unroll
+        for (int r = 0; r < NR; r++) s.preE[r][base + sidx] = Ex[r];
         s.preP[base + sidx] = Px;
-        double e = s.aggE[base + sidx], p = s.aggP[base + sidx];
-        Ex = e + p * Ex;
+        const double p = s.aggP[base + sidx];
+#pragma unroll
+        for (int r = 0; r < NR; r++) Ex[r] = s.aggE[r][base + sidx] + p * Ex[r];
         Px = p * Px;
     }
 }
@@ -174,135 +194,222 @@ __device__ __forceinline__ double xl_tab(const double *tab, const XFTables &tb, 
     return tb.inner[mat][which];
 }
 
-// Exact split Thomas solve of operator OP over the core rows of tile t.
-// Results go to global memory (column pointer gout, row stride ny) and/or
-// back into the tile's core rows (tout).  `par` alternates between calls so
-// that consecutive solves exchange carries through different arrays; the
-// caller issues a cluster barrier before reading results of other CTAs.
-template <int W, int OP>
+// Inflow of this CTA from the CTAs before it (forward, dir = 0) or after it
+// (backward, dir = 1): their totals (E, P) composed over at most `hops`
+// neighbours.  The omitted farther totals enter multiplied by the products
+// of the `hops` nearer chunks, which the host keeps below 2^-60 (hops = C
+// chains through the whole cluster when it cannot).  With hops <= 2 both
+// remote loads are issued at once.
+template <int W, int NR>
+__device__ __forceinline__ void xl_inflow(const XFArgs &a, cg::cluster_group &cluster, double *cta,
+                                          int crank, int dir, int lane, double cin[NR])
+{
+#pragma unroll
+    for (int r = 0; r < NR; r++) cin[r] = 0.0;
+    const int h = a.hops;
+    if (h <= 2) {
+        double e[2][NR], p[2];
+#pragma unroll
+        for (int k = 0; k < 2; k++) {  // k = 0: nearest neighbour
+            const int c2 = dir == 0 ? crank - 1 - k : crank + 1 + k;
+            p[k] = 0.0;
+#pragma unroll
+            for (int r = 0; r < NR; r++) e[k][r] = 0.0;
+            if (k < h && c2 >= 0 && c2 < a.C) {
+                const double *rc = cluster.map_shared_rank(cta, c2);
+                const int off = dir == 0 ? 0 : 3;
+#pragma unroll
+                for (int r = 0; r < NR; r++) e[k][r] = rc[(off + r) * W + lane];
+                p[k] = rc[(off + 2) * W + lane];
+            }
+        }
+#pragma unroll
+        for (int r = 0; r < NR; r++) cin[r] = e[0][r] + p[0] * e[1][r];
+        return;
+    }
+    // the whole chain, farthest first
+    if (dir == 0) {
+        for (int c2 = 0; c2 < crank; c2++) {
+            const double *rc = cluster.map_shared_rank(cta, c2);
+            const double pp = rc[2 * W + lane];
+#pragma unroll
+            for (int r = 0; r < NR; r++) cin[r] = rc[r * W + lane] + pp * cin[r];
+        }
+    } else {
+        for (int c2 = a.C - 1; c2 > crank; c2--) {
+            const double *rc = cluster.map_shared_rank(cta, c2);
+            const double pp = rc[5 * W + lane];
+#pragma unroll
+            for (int r = 0; r < NR; r++) cin[r] = rc[(3 + r) * W + lane] + pp * cin[r];
+        }
+    }
+}
+
+// Exact split Thomas solve over the core rows of the tile(s), NR = 1 or 2
+// systems with the same matrix: operator OP0 on tile t0 and (NR = 2)
+// operator OP1 on tile t1.  Results go to global memory (column pointers
+// g0/g1, row stride ny) and/or, for one system, back into the tile's core
+// rows (tout).  `par` alternates between calls so that consecutive solves
+// exchange carries through different arrays; the caller issues a cluster
+// barrier before reading results of other CTAs.
+template <int W, int OP0, int OP1, int NR>
 __device__ void xl_solve(const XFArgs &a, const XLSmem &s, cg::cluster_group &cluster,
-                         const double *t, double *gout, double *tout, int Rc, long r0, int crank,
-                         int par)
+                         const double *t0, const double *t1, double *g0, double *g1, double *tout,
+                         int Rc, long r0, int crank, int par)
 {
     constexpr int NSUB = XLGeom<W>::NSUB;
-    constexpr int MAT = OP == XOP_F ? 1 : 0;
+    constexpr int MAT = OP0 == XOP_F ? 1 : 0;
+    static_assert(NR == 1 || (OP1 != XOP_F && MAT == 0), "paired systems share the matrix");
     const int tid = threadIdx.x, lane = tid % W, sub = tid / W;
     const int ai = lane * (NSUB + 1) + sub;  // this thread's aggregate slot
     const long nx = a.nx, ny = a.ny;
     const int la = sub * XL_S;
-    const bool edge = (r0 + la < XF_EDGE) || (r0 + la + XL_S > nx - XF_EDGE);
+    // interior sub-chunk: constant factors, branch-free stencils, no row checks
+    const bool fast = !((r0 + la < XF_EDGE) || (r0 + la + XL_S > nx - XF_EDGE)) && la + XL_S <= Rc;
     const double m_in = a.tb.inner[MAT][0], ib_in = a.tb.inner[MAT][1], g_in = a.tb.inner[MAT][2];
     double *cta = s.cta[par];
-    double y[XL_S];
+    const bool same = NR == 2 && t1 == t0;
+    double y[NR][XL_S];
 
     // ---- forward recurrence with zero inflow ------------------------------
-    double yv = 0.0, P = 1.0;
-    {
-        const double *tw = t + (XL_H - 3) * W + lane;  // tw[r * W] = input of local row r - 3
+    double yv[NR], P = 1.0;
+#pragma unroll
+    for (int r = 0; r < NR; r++) yv[r] = 0.0;
+    if (fast) {
+        const double *tw = t0 + (XL_H - 3) * W + lane;  // tw[r * W] = input of local row r - 3
         double w0 = tw[(la + 0) * W], w1 = tw[(la + 1) * W], w2 = tw[(la + 2) * W];
         double w3 = tw[(la + 3) * W], w4 = tw[(la + 4) * W], w5 = tw[(la + 5) * W];
-        if (!edge) {  // interior rows: constant factors, branch-free stencil
+        const double *tv = (NR == 2 ? t1 : t0) + (XL_H - 3) * W + lane;
+        double v0 = 0, v1 = 0, v2 = 0, v3 = 0, v4 = 0, v5 = 0;
+        if (NR == 2 && !same) {
+            v0 = tv[(la + 0) * W]; v1 = tv[(la + 1) * W]; v2 = tv[(la + 2) * W];
+            v3 = tv[(la + 3) * W]; v4 = tv[(la + 4) * W]; v5 = tv[(la + 5) * W];
+        }
 #pragma unroll
-            for (int k = 0; k < XL_S; k++) {
-                const int l = la + k;
-                double w6 = tw[(l + 6) * W];
-                double rhs = xl_rhs<OP>(a.st[OP], w0, w1, w2, w3, w4, w5, w6);
-                if (l < Rc) {
-                    yv = rhs - m_in * yv;
-                    P *= -m_in;
+        for (int k = 0; k < XL_S; k++) {
+            const int l = la + k;
+            const double w6 = tw[(l + 6) * W];
+            yv[0] = xl_rhs<OP0>(a.st[OP0], w0, w1, w2, w3, w4, w5, w6) - m_in * yv[0];
+            y[0][k] = yv[0];
+            if constexpr (NR == 2) {
+                if (same) {
+                    yv[1] = xl_rhs<OP1>(a.st[OP1], w0, w1, w2, w3, w4, w5, w6) - m_in * yv[1];
+                } else {
+                    const double v6 = tv[(l + 6) * W];
+                    yv[1] = xl_rhs<OP1>(a.st[OP1], v0, v1, v2, v3, v4, v5, v6) - m_in * yv[1];
+                    v0 = v1; v1 = v2; v2 = v3; v3 = v4; v4 = v5; v5 = v6;
                 }
-                y[k] = yv;
-                w0 = w1; w1 = w2; w2 = w3; w3 = w4; w4 = w5; w5 = w6;
+                y[NR - 1][k] = yv[NR - 1];
             }
-        } else {      // near a line end: tabulated factors, closure rows
+            w0 = w1; w1 = w2; w2 = w3; w3 = w4; w4 = w5; w5 = w6;
+        }
+        P = a.pw[MAT][0];  // (-m)^XL_S, formed on the host as the rows would form it
+    } else {  // near a line end or past the last row: tabulated factors, closures
+#pragma unroll
+        for (int r = 0; r < NR; r++) {
+            const double *tw = (r == 0 ? t0 : t1) + (XL_H - 3) * W + lane;
+            double w0 = tw[(la + 0) * W], w1 = tw[(la + 1) * W], w2 = tw[(la + 2) * W];
+            double w3 = tw[(la + 3) * W], w4 = tw[(la + 4) * W], w5 = tw[(la + 5) * W];
+            const XStencil &st = a.st[r == 0 ? OP0 : OP1];
+            double pp = 1.0;
 #pragma unroll
             for (int k = 0; k < XL_S; k++) {
                 const int l = la + k;
                 const long gr = r0 + l;
                 double w6 = tw[(l + 6) * W];
                 if (l < Rc) {
-                    double rhs = stencil(a.st[OP], w0, w1, w2, w3, w4, w5, w6, gr, nx);
+                    double rhs = stencil(st, w0, w1, w2, w3, w4, w5, w6, gr, nx);
                     double m = xl_tab(s.tab, a.tb, MAT, 0, gr, nx);
-                    yv = rhs - m * yv;
-                    P *= -m;
+                    yv[r] = rhs - m * yv[r];
+                    pp *= -m;
                 }
-                y[k] = yv;
+                y[r][k] = yv[r];
                 w0 = w1; w1 = w2; w2 = w3; w3 = w4; w4 = w5; w5 = w6;
             }
+            P = pp;
         }
     }
-    s.aggE[ai] = yv;
+#pragma unroll
+    for (int r = 0; r < NR; r++) s.aggE[r][ai] = yv[r];
     s.aggP[ai] = P;
     __syncthreads();
-    xl_scan<W>(s, cta, 0, false);
+    xl_scan<W, NR>(s, cta, 0, false);
     cluster.sync();
 
     // ---- forward inflow and fix-up; backward recurrence with zero inflow --
-    double cin = 0.0;
-    for (int c2 = 0; c2 < crank; c2++) {
-        const double *rc = cluster.map_shared_rank(cta, c2);
-        cin = rc[lane] + rc[W + lane] * cin;
-    }
-    double d = s.preE[ai] + s.preP[ai] * cin;
-    double xv = 0.0, Q = 1.0;
-    if (!edge) {
+    double cin[NR];
+    xl_inflow<W, NR>(a, cluster, cta, crank, 0, lane, cin);
+    double xv[NR], Q = 1.0;
+    {
+        const double pP = s.preP[ai];
 #pragma unroll
-        for (int k = 0; k < XL_S; k++) {
-            if (la + k < Rc) {
-                d *= -m_in;
-                y[k] += d;
-            }
-        }
+        for (int r = 0; r < NR; r++) {
+            double d = s.preE[r][ai] + pP * cin[r];
+            if (fast) {
 #pragma unroll
-        for (int k = XL_S - 1; k >= 0; k--) {
-            if (la + k < Rc) {
-                xv = y[k] * ib_in - g_in * xv;
-                Q *= -g_in;
-                y[k] = xv;
-            }
-        }
-    } else {
+                for (int k = 0; k < XL_S; k++) {
+                    d *= -m_in;
+                    y[r][k] += d;
+                }
+                double x = 0.0;
 #pragma unroll
-        for (int k = 0; k < XL_S; k++) {
-            const int l = la + k;
-            if (l < Rc) {
-                d *= -xl_tab(s.tab, a.tb, MAT, 0, r0 + l, nx);
-                y[k] += d;
-            }
-        }
+                for (int k = XL_S - 1; k >= 0; k--) {
+                    x = y[r][k] * ib_in - g_in * x;
+                    y[r][k] = x;
+                }
+                xv[r] = x;
+                Q = a.pw[MAT][1];  // (-g)^XL_S
+            } else {
 #pragma unroll
-        for (int k = XL_S - 1; k >= 0; k--) {
-            const int l = la + k;
-            if (l < Rc) {
-                double g = xl_tab(s.tab, a.tb, MAT, 2, r0 + l, nx);
-                xv = y[k] * xl_tab(s.tab, a.tb, MAT, 1, r0 + l, nx) - g * xv;
-                Q *= -g;
-                y[k] = xv;
+                for (int k = 0; k < XL_S; k++) {
+                    const int l = la + k;
+                    if (l < Rc) {
+                        d *= -xl_tab(s.tab, a.tb, MAT, 0, r0 + l, nx);
+                        y[r][k] += d;
+                    }
+                }
+                double x = 0.0, qq = 1.0;
+#pragma unroll
+                for (int k = XL_S - 1; k >= 0; k--) {
+                    const int l = la + k;
+                    if (l < Rc) {
+                        double g = xl_tab(s.tab, a.tb, MAT, 2, r0 + l, nx);
+                        x = y[r][k] * xl_tab(s.tab, a.tb, MAT, 1, r0 + l, nx) - g * x;
+                        qq *= -g;
+                        y[r][k] = x;
+                    }
+                }
+                xv[r] = x;
+                Q = qq;
             }
         }
     }
     __syncthreads();  // everyone has read preE/preP before the scan rewrites them
-    s.aggE[ai] = xv;
+#pragma unroll
+    for (int r = 0; r < NR; r++) s.aggE[r][ai] = xv[r];
     s.aggP[ai] = Q;
     __syncthreads();
-    xl_scan<W>(s, cta, 2, true);
+    xl_scan<W, NR>(s, cta, 3, true);
     cluster.sync();
 
     // ---- backward inflow, fix-up and results -------------------------------
-    double cb = 0.0;
-    for (int c2 = a.C - 1; c2 > crank; c2--) {
-        const double *rc = cluster.map_shared_rank(cta, c2);
-        cb = rc[2 * W + lane] + rc[3 * W + lane] * cb;
-    }
-    d = s.preE[ai] + s.preP[ai] * cb;
+    double cb[NR];
+    xl_inflow<W, NR>(a, cluster, cta, crank, 1, lane, cb);
+    const double pQ = s.preP[ai];
 #pragma unroll
-    for (int k = XL_S - 1; k >= 0; k--) {
-        const int l = la + k;
-        if (l < Rc) {
-            d *= edge ? -xl_tab(s.tab, a.tb, MAT, 2, r0 + l, nx) : -g_in;
-            double v = y[k] + d;
-            if (gout) gout[(r0 + l) * ny] = v;
-            if (tout) tout[(l + XL_H) * W + lane] = v;
+    for (int r = 0; r < NR; r++) {
+        double d = s.preE[r][ai] + pQ * cb[r];
+        double *g = r == 0 ? g0 : g1;
+        if (g) g += (size_t)r0 * ny;
+#pragma unroll
+        for (int k = XL_S - 1; k >= 0; k--) {
+            const int l = la + k;
+            if (l < Rc) {
+                d *= fast ? -g_in : -xl_tab(s.tab, a.tb, MAT, 2, r0 + l, nx);
+                double v = y[r][k] + d;
+                if (g) g[(size_t)l * ny] = v;
+                if (NR == 1 && tout) tout[(l + XL_H) * W + lane] = v;
+            }
         }
     }
 }
@@ -429,15 +536,18 @@ xline_kernel(XFArgs a, const __grid_constant__ CUtensorMap tm_big,
         double *t = s.tile[b];
         if (a.single_op >= 0) {  // one operator per field
             double *g = (a.out1 && col) ? a.out1 + (size_t)f * plane + j0 + lane : nullptr;
-            if (a.single_op == XOP_F) xl_solve<W, XOP_F>(a, s, cluster, t, g, nullptr, Rc, r0, crank, par);
-            else if (a.single_op == XOP_D1) xl_solve<W, XOP_D1>(a, s, cluster, t, g, nullptr, Rc, r0, crank, par);
-            else xl_solve<W, XOP_D2>(a, s, cluster, t, g, nullptr, Rc, r0, crank, par);
+            if (a.single_op == XOP_F)
+                xl_solve<W, XOP_F, XOP_F, 1>(a, s, cluster, t, t, g, nullptr, nullptr, Rc, r0, crank, par);
+            else if (a.single_op == XOP_D1)
+                xl_solve<W, XOP_D1, XOP_D1, 1>(a, s, cluster, t, t, g, nullptr, nullptr, Rc, r0, crank, par);
+            else
+                xl_solve<W, XOP_D2, XOP_D2, 1>(a, s, cluster, t, t, g, nullptr, nullptr, Rc, r0, crank, par);
             par ^= 1;
             continue;
         }
         if (a.fout) {
             double *g = col ? a.fout + (size_t)v * plane + j0 + lane : nullptr;
-            xl_solve<W, XOP_F>(a, s, cluster, t, g, t, Rc, r0, crank, par);
+            xl_solve<W, XOP_F, XOP_F, 1>(a, s, cluster, t, t, g, nullptr, t, Rc, r0, crank, par);
             par ^= 1;
             cluster.sync();  // every CTA's tile holds its filtered core rows
             // halo rows of the filtered line from the neighbouring CTAs
@@ -455,18 +565,18 @@ xline_kernel(XFArgs a, const __grid_constant__ CUtensorMap tm_big,
             __syncthreads();
         }
         if (!a.out1) continue;
-        xl_solve<W, XOP_D1>(a, s, cluster, t, col ? a.out1 + (size_t)v * plane + j0 + lane : nullptr,
-                            nullptr, Rc, r0, crank, par);
-        par ^= 1;
+        double *g1 = col ? a.out1 + (size_t)v * plane + j0 + lane : nullptr;
         double *g2 = nullptr;
         if (a.out2a && v >= a.d2a_lo && v < a.d2a_lo + 3)
             g2 = a.out2a + (size_t)(v - a.d2a_lo) * plane + j0 + lane;
         else if (a.out2b && v >= a.d2b_lo && v < a.d2b_lo + 3)
             g2 = a.out2b + (size_t)(v - a.d2b_lo) * plane + j0 + lane;
-        if (g2) {
-            xl_solve<W, XOP_D2>(a, s, cluster, t, col ? g2 : nullptr, nullptr, Rc, r0, crank, par);
-            par ^= 1;
-        }
+        if (g2)  // d/dx and d2/dx2 share the matrix: one paired solve
+            xl_solve<W, XOP_D1, XOP_D2, 2>(a, s, cluster, t, t, g1, col ? g2 : nullptr, nullptr, Rc,
+                                           r0, crank, par);
+        else
+            xl_solve<W, XOP_D1, XOP_D1, 1>(a, s, cluster, t, t, g1, nullptr, nullptr, Rc, r0, crank, par);
+        par ^= 1;
     }
 
     if (a.outE) {
@@ -475,21 +585,25 @@ xline_kernel(XFArgs a, const __grid_constant__ CUtensorMap tm_big,
         __threadfence();
         cluster.sync();
         const double *u = a.in;
-        for (int e = 0; e < 2; e++) {
-            double *t = s.tile[e];
-            for (int idx = tid; idx < (Rc + 2 * XL_H) * W; idx += XL_T) {
-                int r = idx / W, c = idx % W;
-                if (c < ncols) {
-                    size_t o = (size_t)wrap(r0 - XL_H + r, nx) * ny + j0 + c;
-                    t[idx] = e == 0 ? u[UX * plane + o] * u[BZ * plane + o] - u[UZ * plane + o] * u[BX * plane + o]
-                                    : u[UY * plane + o] * u[BX * plane + o] - u[UX * plane + o] * u[BY * plane + o];
-                }
+        for (int idx = tid; idx < (Rc + 2 * XL_H) * W; idx += XL_T) {
+            const int r = idx / W, c = idx % W;
+            if (c < ncols) {
+                long gr = r0 - XL_H + r;  // within [-XL_H, nx + XL_H): one wrap at most
+                gr = gr < 0 ? gr + nx : (gr >= nx ? gr - nx : gr);
+                const size_t o = (size_t)gr * ny + j0 + c;
+                const double ux = u[UX * plane + o], uy = u[UY * plane + o], uz = u[UZ * plane + o];
+                const double bx = u[BX * plane + o], by = u[BY * plane + o], bz = u[BZ * plane + o];
+                s.tile[0][idx] = ux * bz - uz * bx;
+                s.tile[1][idx] = uy * bx - ux * by;
             }
-            __syncthreads();
-            xl_solve<W, XOP_D1>(a, s, cluster, t, col ? a.outE + (size_t)e * plane + j0 + lane : nullptr,
-                                nullptr, Rc, r0, crank, par);
-            par ^= 1;
         }
+        __syncthreads();
+        // Ey and Ez share the matrix: one paired solve
+        xl_solve<W, XOP_D1, XOP_D1, 2>(a, s, cluster, s.tile[0], s.tile[1],
+                                       col ? a.outE + j0 + lane : nullptr,
+                                       col ? a.outE + plane + j0 + lane : nullptr, nullptr, Rc, r0,
+                                       crank, par);
+        par ^= 1;
     }
     cluster.sync();  // peers may still read this CTA's shared memory
 }
@@ -597,6 +711,57 @@ int xline_setup(Ctx *c)
     c->xf_W = W;
     c->xf_C = C;
     c->xf_R = (int)R;
+    // Interior products of a full sub-chunk, (-m)^XL_S and (-g)^XL_S, formed
+    // in the order the device forms them row by row.
+    for (int mat = 0; mat < 2; mat++) {
+        double pm = 1.0, pg = 1.0;
+        for (int k = 0; k < XL_S; k++) {
+            pm *= -c->xf_inner[mat][0];
+            pg *= -c->xf_inner[mat][2];
+        }
+        c->xf_pw[mat][0] = pm;
+        c->xf_pw[mat][1] = pg;
+    }
+    // Carries between CTAs: the inflow of a CTA is composed over its `hops`
+    // nearest neighbours; the totals beyond enter multiplied by the products
+    // of those chunks' Thomas factors.  Take the fewest hops (at least 2)
+    // that keep every such product below 2^-60 in both directions, else
+    // chain through the whole cluster.
+    {
+        std::vector<double> h[2][2];
+        const int ops[2] = {XOP_D1, XOP_F};
+        for (int mat = 0; mat < 2; mat++) {
+            const double *dev[2] = {c->xt[ops[mat]].m, c->xt[ops[mat]].g};
+            for (int w = 0; w < 2; w++) {
+                h[mat][w].resize(n);
+                MHD_CUDA_TRY(cudaMemcpy(h[mat][w].data(), dev[w], sizeof(double) * n,
+                                        cudaMemcpyDeviceToHost));
+            }
+        }
+        std::vector<double> cp[2][2];  // |product| of the factors over each chunk
+        for (int mat = 0; mat < 2; mat++)
+            for (int w = 0; w < 2; w++) {
+                cp[mat][w].assign(C, 1.0);
+                for (long i = 0; i < n; i++) cp[mat][w][i / R] *= std::fabs(h[mat][w][i]);
+            }
+        int hops = 2;
+        for (; hops < C; hops++) {
+            bool ok = true;
+            for (int mat = 0; mat < 2 && ok; mat++)
+                for (int w = 0; w < 2 && ok; w++)
+                    for (int cc = 0; cc < C && ok; cc++) {
+                        // w = 0: forward inflow of cc from cc-1 .. cc-hops;
+                        // w = 1: backward inflow from cc+1 .. cc+hops
+                        const int far = w == 0 ? cc - hops - 1 : cc + hops + 1;
+                        if (far < 0 || far >= C) continue;  // the chain is complete
+                        double p = 1.0;
+                        for (int k = 1; k <= hops; k++) p *= cp[mat][w][w == 0 ? cc - k : cc + k];
+                        if (p >= std::ldexp(1.0, -60)) ok = false;
+                    }
+            if (ok) break;
+        }
+        c->xf_hops = hops >= C ? C : hops;
+    }
     const long rows = (long)c->nvar * n;
     if ((rc = xl_tensor_map(&c->xl_tmap_big, c->arr[MHDGPU_UU], rows, c->ny, W, XL_BOX))) return rc;
     if ((rc = xl_tensor_map(&c->xl_tmap_unit, c->arr[MHDGPU_UU], rows, c->ny, W, W == 8 ? 2 : 1)))
@@ -632,6 +797,8 @@ int launch_xline(Ctx *c, const XFArgs &proto, double bytes)
     a.ny = c->ny;
     a.R = c->xf_R;
     a.C = c->xf_C;
+    a.hops = c->xf_hops;
+    std::memcpy(a.pw, c->xf_pw, sizeof a.pw);
     a.flag = c->dflag;
     const int W = c->xf_W;
     const int ntiles = (int)((c->ny + W - 1) / W);
