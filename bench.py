@@ -158,14 +158,19 @@ def algorithmic_model_bytes():
 
 
 def traffic_per_launch(kclass):
-    """dram bytes per launch of a kernel class from the committed ncu summary
-    (profiles/ncu_traffic.json), or None."""
-    path = os.path.join(ROOT, "profiles", "ncu_traffic.json")
+    """DRAM bytes per launch of a kernel class at the bench workload, from the
+    committed ncu summary profiles/ncu_traffic.txt (lines `class bytes`), or
+    None when it has no figure for the class."""
+    path = os.path.join(ROOT, "profiles", "ncu_traffic.txt")
     try:
         with open(path) as f:
-            return float(json.load(f)[kclass]["dram_bytes_per_launch"])
-    except Exception:
-        return None
+            for line in f:
+                parts = line.split()
+                if len(parts) >= 2 and parts[0] == kclass:
+                    return float(parts[1])
+    except OSError:
+        pass
+    return None
 
 
 def run_ours(args):
