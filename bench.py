@@ -173,6 +173,23 @@ def traffic_per_launch(kclass):
     return None
 
 
+def max_over_ranks(x, dist, device):
+    """The largest of the ranks' values of x (every rank calls it, in the
+    same order); x itself without a process group."""
+    if dist is None:
+        return x
+    import torch
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replica_value(world, cells, steps, seconds):
+    """Whole-job cell-updates/s of `world` independent replicas of `cells`
+    cells advanced `steps` steps, timed by the slowest rank (seconds)."""
+    return world * cells * steps / seconds
+
+
 def run_ours(args):
     rank, local, world = env_rank()
     import numpy as np
@@ -190,9 +207,17 @@ def run_ours(args):
     from mhd2dcfdfftw_open_b200.solver import Domain
 
     nx, ny = args.nx, args.ny
-    p, uu = ic.alfvenic_turbulence(nx, ny)
+    if args.workload == "parametric":  # parametric decay of an Alfven pump, dt 5e-4
+        p, uu = ic.parametric_decay(nx, ny)
+        dt = 5e-4
+    else:                              # Alfvenic turbulence, dt 2e-4
+        p, uu = ic.alfvenic_turbulence(nx, ny)
+        dt = DT
     fused = args.path == "fused"
     dom = Domain(p, uu, device=local)
+    mixed = args.precision == "mixed"
+    if mixed:
+        dom.set_precision(True)
     stream = torch.cuda.ExternalStream(dom.stream_handle(), device=local)
 
     def barrier():
@@ -200,7 +225,7 @@ def run_ours(args):
             dist.barrier()
 
     # warm-up steps (untimed)
-    dom.steps(args.warmup, DT, fused=fused)
+    dom.steps(args.warmup, dt, fused=fused)
     barrier()
     torch.cuda.synchronize()
     dom.synchronize()
@@ -212,7 +237,7 @@ def run_ours(args):
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
     e0.record(stream)
-    dom.steps(args.steps, DT, fused=fused)
+    dom.steps(args.steps, dt, fused=fused)
     e1.record(stream)
     e1.synchronize()
     torch.cuda.synchronize()
@@ -222,12 +247,9 @@ def run_ours(args):
     ms = e0.elapsed_time(e1)
     prof = dom.profile_read()
     dom.profile(False)
-    if dist is not None:
-        t = torch.tensor([ms], dtype=torch.float64, device=f"cuda:{local}")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
+    ms = max_over_ranks(ms, dist, f"cuda:{local}")
     cells = float(nx) * ny
-    value = world * cells * args.steps / (ms / 1e3)
+    value = replica_value(world, cells, args.steps, ms / 1e3)
 
     # end to end through the C ABI with host buffers: every step uploads the
     # state from pinned host memory, advances one RK3 step and reads the state
@@ -237,21 +259,38 @@ def run_ours(args):
     h_out = torch.empty_like(h_in).pin_memory()
     nin, nout = h_in.numpy(), h_out.numpy()
     dom.set("uu", nin)
-    dom.steps(1, DT, fused=fused)
+    dom.steps(1, dt, fused=fused)
     barrier()
     t0 = time.perf_counter()
     for _ in range(ke):
         dom.set("uu", nin)
-        dom.steps(1, DT, fused=fused)
+        dom.steps(1, dt, fused=fused)
         dom.get("uu", out=nout)
     t_e2e = time.perf_counter() - t0
-    if dist is not None:
-        t = torch.tensor([t_e2e], dtype=torch.float64, device=f"cuda:{local}")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        t_e2e = float(t.item())
-    e2e = world * cells * ke / t_e2e
+    t_e2e = max_over_ranks(t_e2e, dist, f"cuda:{local}")
+    e2e = replica_value(world, cells, ke, t_e2e)
     nbytes = nin.nbytes
     dom.close()
+
+    # mixed precision: its error against the FP64 steps from the same state
+    mixed_error = None
+    if mixed:
+        runs = []
+        for mx in (False, True):
+            with Domain(p, uu, device=local) as d:
+                d.set_precision(mx)
+                d.steps(args.warmup + args.steps, dt, fused=fused)
+                runs.append(d.get("uu"))
+        ref, mix = runs
+        per = []
+        for v in range(ref.shape[0]):
+            den = float(np.linalg.norm(ref[v]))
+            if den < 1e-8 * float(np.linalg.norm(ref)):
+                den = float(np.linalg.norm(ref))
+            per.append(float(np.linalg.norm(mix[v] - ref[v]) / den))
+        mixed_error = {"rel_l2_per_field": per, "rel_l2_max": max(per),
+                       "steps": args.warmup + args.steps,
+                       "against": "FP64 fused steps on the GPU (which match the reference to 1e-12)"}
 
     if rank != 0:
         if dist is not None:
@@ -273,9 +312,13 @@ def run_ours(args):
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": "f64", "data": "synthetic (seeded Alfvenic turbulence IC, seed 1)",
-        "config": {"workload": f"alfvenic_turbulence_{nx}x{ny}_fp64", "nx": nx, "ny": ny,
-                   "dt": DT, "path": args.path, "parallelism": f"replicas{world}",
+        "dtype": "f32 sweeps/FFT/fluxes, f64 state" if mixed else "f64",
+        "data": ("synthetic (seeded parametric-decay IC, seed 3)" if args.workload == "parametric"
+                 else "synthetic (seeded Alfvenic turbulence IC, seed 1)"),
+        "config": {"workload": f"{'parametric_decay' if args.workload == 'parametric' else 'alfvenic_turbulence'}"
+                               f"_{nx}x{ny}_{'mixed' if mixed else 'fp64'}",
+                   "nx": nx, "ny": ny, "precision": args.precision,
+                   "dt": dt, "path": args.path, "parallelism": f"replicas{world}",
                    "l2": "inputs larger than L2 (state alone is "
                          f"{8 * cells * 8 / 1e9:.2f} GB)"},
         "roofline": roofline,
@@ -285,6 +328,7 @@ def run_ours(args):
         "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": nbytes,
                 "d2h_bytes_per_step": nbytes, "steps": ke},
         "gpu_launches": launches,
+        **({"mixed_error": mixed_error} if mixed_error else {}),
         "clocks": clocks,
     }
     if world == 1 and not args.no_cpu_baseline:
@@ -342,6 +386,8 @@ def main():
     ap.add_argument("--ny", type=int, default=4096)
     ap.add_argument("--e2e-steps", type=int, default=5)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--precision", choices=["fp64", "mixed"], default="fp64")
+    ap.add_argument("--workload", choices=["turbulence", "parametric"], default="turbulence")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

@@ -114,6 +114,20 @@ int mhdgpu_steps(mhdgpu_ctx *ctx, int nsteps, double dt_fixed, double *dt_io);
 /* Same steps through the fused two-pass stage (x pass + y pass per stage). */
 int mhdgpu_steps_fused(mhdgpu_ctx *ctx, int nsteps, double dt_fixed, double *dt_io);
 
+/* Arithmetic of mhdgpu_steps_fused (no counterpart in the reference, which
+ * computes in FP64 only).  MHDGPU_PRECISION_FP64 (the default) follows the
+ * reference's numerics.  MHDGPU_PRECISION_MIXED keeps the state, dudtRK,
+ * the RK3 update, the CFL time step and the right-hand sides of the compact
+ * schemes in FP64, and runs the tridiagonal sweeps, the FFT butterflies and
+ * the fluxes in FP32; the derivatives are stored as FP32 and the x and y
+ * filters are applied as an FP32 change added to the FP64 state.  After
+ * mixed steps the derivative arrays hold FP32 scratch (mhdgpu_check_divb then
+ * returns MHDGPU_ERR_UNSUPPORTED until an FP64 step has run).  Mixed
+ * precision needs the fused path: 16 <= ny <= 4096, a grid the fused x pass
+ * tiles, and divBcleaning 0 or 2; otherwise MHDGPU_ERR_UNSUPPORTED. */
+enum { MHDGPU_PRECISION_FP64 = 0, MHDGPU_PRECISION_MIXED = 1 };
+int mhdgpu_set_precision(mhdgpu_ctx *ctx, int precision);
+
 /* --- diagnostics -------------------------------------------------------- */
 /* total energy, cross helicity (sums times dx*dy) and max|divB| of the last
  * computed derivatives; *finite = 0 if the state holds NaN/Inf or rho,p<=0 */

@@ -351,6 +351,7 @@ extern "C" int mhdgpu_check_divb(mhdgpu_ctx *h, double *maxdivb)
 {
     CTX_OR_FAIL(h);
     if (!maxdivb) return mhd_set_error(MHDGPU_ERR_INVALID);
+    if (c->deriv_fp32) return mhd_set_error(MHDGPU_ERR_UNSUPPORTED);  // FP32 scratch
     return mhd::launch_max_divb(c, maxdivb);
 }
 
@@ -419,6 +420,7 @@ extern "C" int mhdgpu_steps(mhdgpu_ctx *h, int nsteps, double dt_fixed, double *
 {
     CTX_OR_FAIL(h);
     if (nsteps < 0) return mhd_set_error(MHDGPU_ERR_INVALID);
+    if (nsteps > 0) c->deriv_fp32 = 0;  // every stage rewrites the derivatives in FP64
     TRY(settle(c));
     double dt = dt_io ? *dt_io : 0.0;
     TRY(next_dt(h, c, dt_fixed, &dt));
@@ -441,7 +443,10 @@ extern "C" int mhdgpu_steps_fused(mhdgpu_ctx *h, int nsteps, double dt_fixed, do
 {
     CTX_OR_FAIL(h);
     if (nsteps < 0) return mhd_set_error(MHDGPU_ERR_INVALID);
+    if (c->mixed && (c->p.divBcleaning == 1 || c->xf_W == 0 || !mhd::yrow_supported(c)))
+        return mhd_set_error(MHDGPU_ERR_UNSUPPORTED);
     if (c->p.divBcleaning == 1 || c->xf_W == 0) return mhdgpu_steps(h, nsteps, dt_fixed, dt_io);
+    if (nsteps > 0) c->deriv_fp32 = c->mixed;
     const bool need_dt = dt_fixed <= 0 || c->p.divBcleaning == 2;
     double dt = dt_io ? *dt_io : 0.0;
     if (need_dt) TRY(settle(c));
@@ -457,6 +462,18 @@ extern "C" int mhdgpu_steps_fused(mhdgpu_ctx *h, int nsteps, double dt_fixed, do
     if (dt_io) *dt_io = dt;
     MHD_CUDA_TRY(cudaStreamSynchronize(c->stream));
     return check_flag(c);
+}
+
+extern "C" int mhdgpu_set_precision(mhdgpu_ctx *h, int precision)
+{
+    CTX_OR_FAIL(h);
+    if (precision != MHDGPU_PRECISION_FP64 && precision != MHDGPU_PRECISION_MIXED)
+        return mhd_set_error(MHDGPU_ERR_INVALID);
+    if (precision == MHDGPU_PRECISION_MIXED &&
+        (c->p.divBcleaning == 1 || c->xf_W == 0 || !mhd::yrow_supported(c)))
+        return mhd_set_error(MHDGPU_ERR_UNSUPPORTED);
+    c->mixed = precision == MHDGPU_PRECISION_MIXED;
+    return MHDGPU_OK;
 }
 
 extern "C" int mhdgpu_diagnostics(mhdgpu_ctx *h, double *energy, double *cross_helicity, int *finite)

@@ -66,6 +66,11 @@ struct Ctx {
     // y spectral tables
     double2 *tw;                 // exp(-2 pi i m / ny), m < ny
     double *ysym_d1, *ysym_d2, *ysym_f;  // per signed wavenumber, ny each
+    // FP32 copies for the mixed-precision stage: twiddles, d/dy, d2/dy2 and
+    // filter-minus-identity symbols, ny float2 each
+    float2 *ytab32;
+    int mixed;       // fused steps in mixed precision (FP32 operators, FP64 state)
+    int deriv_fp32;  // the derivative arrays hold FP32 scratch of mixed steps
     // scalars on the device: [0] dt, [1] Ch, [2] Cp, [3..] scratch
     double *dscal;
     double *dred;                // block partials of reductions
@@ -93,6 +98,7 @@ struct Ctx {
     int xf_W, xf_C, xf_R;
     int xf_hops;          // CTAs whose totals enter an inflow of the fused x pass
     double xf_pw[2][2];   // interior sub-chunk products (-m)^S, (-g)^S per matrix
+    double xf_alphaF[2];  // filter matrix off-diagonal: interior, edge rows
     CUtensorMap xl_tmap_big, xl_tmap_unit;  // uu as [nvar*nx rows][ny] for the x pass
 };
 
@@ -135,4 +141,5 @@ void xline_free(Ctx *c);
 int fused_setup(Ctx *c);
 void fused_free(Ctx *c);
 int fused_stage(Ctx *c, int iRK, int first_stage_of_run, int last_stage);
+bool yrow_supported(const Ctx *c);
 }  // namespace mhd

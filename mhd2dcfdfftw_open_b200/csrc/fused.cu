@@ -40,7 +40,10 @@ static int fused_x_pass(Ctx *c)
     a.out2b = (p.resistivity > 0 || p.Hall == 1) ? c->arr[MHDGPU_D2BDX2] : nullptr;
     a.d2b_lo = BX;
     a.single_op = -1;
-    a.outE = c->arr[MHDGPU_DEDX] + (size_t)c->nx * c->ny;  // dEdx[1], dEdx[2]
+    // dEdx[1], dEdx[2]: one plane into the array, in the stored element type
+    const size_t plane = (size_t)c->nx * c->ny;
+    a.outE = c->mixed ? reinterpret_cast<double *>(reinterpret_cast<float *>(c->arr[MHDGPU_DEDX]) + plane)
+                      : c->arr[MHDGPU_DEDX] + plane;
     int n2 = (a.out2a ? 3 : 0) + (a.out2b ? 3 : 0);
     double bytes = planeb(c) * (c->nvar + (a.fout ? c->nvar : 0) + c->nvar + n2 + 2);
     return launch_xline(c, a, bytes);

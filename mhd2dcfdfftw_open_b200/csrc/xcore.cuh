@@ -38,6 +38,7 @@ struct XFArgs {
     int R, C;
     int hops;             // CTAs whose totals enter a CTA's inflow (C: all)
     double pw[2][2];      // per matrix: (-m)^XL_S, (-g)^XL_S of the interior
+    double fa_in, fa_sub; // filter matrix off-diagonals: interior, and rows 0 / n-1
     int *flag;
 };
 

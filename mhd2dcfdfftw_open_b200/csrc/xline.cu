@@ -44,6 +44,9 @@ namespace mhd {
 #ifndef MHD_XLINE_ROWS
 #define MHD_XLINE_ROWS 8
 #endif
+#ifndef MHD_XLINE_MINB
+#define MHD_XLINE_MINB 1
+#endif
 constexpr int XL_T = MHD_XLINE_THREADS;  // threads per CTA
 constexpr int XL_S = MHD_XLINE_ROWS;     // rows of a recurrence per thread
 // Halo rows kept on each side of a CTA's rows (the stencils use 3): with 4,
@@ -73,31 +76,34 @@ __host__ __device__ constexpr size_t xl_smem_bytes()
 // Aggregates of the sub-chunk recurrences.  Up to two systems with the same
 // matrix are solved side by side, so they share the products P and carry
 // their own end values E[0], E[1].
+// T is the type of the recurrences (double, or float in the mixed-precision
+// pass); the arrays are sized for doubles either way.
+template <typename T>
 struct XLSmem {
     double *tile[2];
     double *tab;
-    double *aggE[2], *aggP;  // sub-chunk end values and product (zero inflow)
-    double *preE[2], *preP;  // composite of the preceding sub-chunks of the CTA
-    double *cta[2];          // [fwE0, fwE1, fwP, bwE0, bwE1, bwP] x W, alternating between solves
+    T *aggE[2], *aggP;  // sub-chunk end values and product (zero inflow)
+    T *preE[2], *preP;  // composite of the preceding sub-chunks of the CTA
+    T *cta[2];          // [fwE0, fwE1, fwP, bwE0, bwE1, bwP] x W, alternating between solves
     uint64_t *bar;
 };
 
-template <int W>
-__device__ __forceinline__ XLSmem xl_carve(unsigned char *raw)
+template <int W, typename T>
+__device__ __forceinline__ XLSmem<T> xl_carve(unsigned char *raw)
 {
-    XLSmem s;
+    XLSmem<T> s;
     double *p = reinterpret_cast<double *>(raw);
     s.tile[0] = p; p += (size_t)XLGeom<W>::TROWS * W;
     s.tile[1] = p; p += (size_t)XLGeom<W>::TROWS * W;
     s.tab = p; p += 2 * 3 * 2 * XF_EDGE;
-    s.aggE[0] = p; p += xl_aggn<W>();
-    s.aggE[1] = p; p += xl_aggn<W>();
-    s.aggP = p; p += xl_aggn<W>();
-    s.preE[0] = p; p += xl_aggn<W>();
-    s.preE[1] = p; p += xl_aggn<W>();
-    s.preP = p; p += xl_aggn<W>();
-    s.cta[0] = p; p += 6 * W;
-    s.cta[1] = p; p += 6 * W;
+    s.aggE[0] = reinterpret_cast<T *>(p); p += xl_aggn<W>();
+    s.aggE[1] = reinterpret_cast<T *>(p); p += xl_aggn<W>();
+    s.aggP = reinterpret_cast<T *>(p); p += xl_aggn<W>();
+    s.preE[0] = reinterpret_cast<T *>(p); p += xl_aggn<W>();
+    s.preE[1] = reinterpret_cast<T *>(p); p += xl_aggn<W>();
+    s.preP = reinterpret_cast<T *>(p); p += xl_aggn<W>();
+    s.cta[0] = reinterpret_cast<T *>(p); p += 6 * W;
+    s.cta[1] = reinterpret_cast<T *>(p); p += 6 * W;
     s.bar = reinterpret_cast<uint64_t *>(p);
     return s;
 }
@@ -107,8 +113,8 @@ __device__ __forceinline__ XLSmem xl_carve(unsigned char *raw)
 // in order (reversed for the backward sweep), writes the CTA total to
 // cta[off * W ..] and the composite of the preceding sub-chunks to preE/preP.
 // Composition: segment A then B gives (E_B + P_B E_A, P_A P_B).
-template <int W, int NR>
-__device__ __forceinline__ void xl_scan(const XLSmem &s, double *cta, int off, bool reverse)
+template <int W, int NR, typename T>
+__device__ __forceinline__ void xl_scan(const XLSmem<T> &s, T *cta, int off, bool reverse)
 {
     constexpr int NSUB = XLGeom<W>::NSUB;
     // sub-chunks per lane; with fewer sub-chunks than lanes the idle lanes
@@ -118,15 +124,15 @@ __device__ __forceinline__ void xl_scan(const XLSmem &s, double *cta, int off, b
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     if (warp >= W) return;
     const int base = warp * (NSUB + 1);
-    double E[NR], P = 1.0;
+    T E[NR], P = (T)1;
 #pragma unroll
-    for (int r = 0; r < NR; r++) E[r] = 0.0;
+    for (int r = 0; r < NR; r++) E[r] = (T)0;
 #pragma unroll
     for (int jq = 0; jq < K; jq++) {
         int q = lane * K + jq;
         if (q >= NSUB) break;
         int sidx = reverse ? NSUB - 1 - q : q;
-        const double p = s.aggP[base + sidx];
+        const T p = s.aggP[base + sidx];
 #pragma unroll
         for (int r = 0; r < NR; r++) E[r] = s.aggE[r][base + sidx] + p * E[r];
         P = p * P;
@@ -134,24 +140,24 @@ __device__ __forceinline__ void xl_scan(const XLSmem &s, double *cta, int off, b
     // every lane takes part in every shuffle (full mask)
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) {
-        double Eo[NR];
+        T Eo[NR];
 #pragma unroll
         for (int r = 0; r < NR; r++) Eo[r] = __shfl_up_sync(0xffffffffu, E[r], o);
-        const double Po = __shfl_up_sync(0xffffffffu, P, o);
+        const T Po = __shfl_up_sync(0xffffffffu, P, o);
         if (lane >= o) {
 #pragma unroll
             for (int r = 0; r < NR; r++) E[r] = E[r] + P * Eo[r];
             P = P * Po;
         }
     }
-    double Ex[NR];
+    T Ex[NR];
 #pragma unroll
     for (int r = 0; r < NR; r++) {
-        const double e = __shfl_up_sync(0xffffffffu, E[r], 1);
-        Ex[r] = lane == 0 ? 0.0 : e;
+        const T e = __shfl_up_sync(0xffffffffu, E[r], 1);
+        Ex[r] = lane == 0 ? (T)0 : e;
     }
-    const double pxs = __shfl_up_sync(0xffffffffu, P, 1);
-    double Px = lane == 0 ? 1.0 : pxs;
+    const T pxs = __shfl_up_sync(0xffffffffu, P, 1);
+    T Px = lane == 0 ? (T)1 : pxs;
     if (lane == 31) {
 #pragma unroll
         for (int r = 0; r < NR; r++) cta[(off + r) * W + warp] = E[r];
@@ -165,7 +171,7 @@ __device__ __forceinline__ void xl_scan(const XLSmem &s, double *cta, int off, b
 #pragma unroll
         for (int r = 0; r < NR; r++) s.preE[r][base + sidx] = Ex[r];
         s.preP[base + sidx] = Px;
-        const double p = s.aggP[base + sidx];
+        const T p = s.aggP[base + sidx];
 #pragma unroll
         for (int r = 0; r < NR; r++) Ex[r] = s.aggE[r][base + sidx] + p * Ex[r];
         Px = p * Px;
@@ -194,29 +200,36 @@ __device__ __forceinline__ double xl_tab(const double *tab, const XFTables &tb, 
     return tb.inner[mat][which];
 }
 
+// Output element type of a solve: the filter writes the FP64 state, the
+// derivatives are stored in the recurrence type.
+template <int OP, typename T>
+struct XLOut { using type = T; };
+template <typename T>
+struct XLOut<XOP_F, T> { using type = double; };
+
 // Inflow of this CTA from the CTAs before it (forward, dir = 0) or after it
 // (backward, dir = 1): their totals (E, P) composed over at most `hops`
 // neighbours.  The omitted farther totals enter multiplied by the products
 // of the `hops` nearer chunks, which the host keeps below 2^-60 (hops = C
 // chains through the whole cluster when it cannot).  With hops <= 2 both
 // remote loads are issued at once.
-template <int W, int NR>
-__device__ __forceinline__ void xl_inflow(const XFArgs &a, cg::cluster_group &cluster, double *cta,
-                                          int crank, int dir, int lane, double cin[NR])
+template <int W, int NR, typename T>
+__device__ __forceinline__ void xl_inflow(const XFArgs &a, cg::cluster_group &cluster, T *cta,
+                                          int crank, int dir, int lane, T cin[NR])
 {
 #pragma unroll
-    for (int r = 0; r < NR; r++) cin[r] = 0.0;
+    for (int r = 0; r < NR; r++) cin[r] = (T)0;
     const int h = a.hops;
     if (h <= 2) {
-        double e[2][NR], p[2];
+        T e[2][NR], p[2];
 #pragma unroll
         for (int k = 0; k < 2; k++) {  // k = 0: nearest neighbour
             const int c2 = dir == 0 ? crank - 1 - k : crank + 1 + k;
-            p[k] = 0.0;
+            p[k] = (T)0;
 #pragma unroll
-            for (int r = 0; r < NR; r++) e[k][r] = 0.0;
+            for (int r = 0; r < NR; r++) e[k][r] = (T)0;
             if (k < h && c2 >= 0 && c2 < a.C) {
-                const double *rc = cluster.map_shared_rank(cta, c2);
+                const T *rc = cluster.map_shared_rank(cta, c2);
                 const int off = dir == 0 ? 0 : 3;
 #pragma unroll
                 for (int r = 0; r < NR; r++) e[k][r] = rc[(off + r) * W + lane];
@@ -230,15 +243,15 @@ __device__ __forceinline__ void xl_inflow(const XFArgs &a, cg::cluster_group &cl
     // the whole chain, farthest first
     if (dir == 0) {
         for (int c2 = 0; c2 < crank; c2++) {
-            const double *rc = cluster.map_shared_rank(cta, c2);
-            const double pp = rc[2 * W + lane];
+            const T *rc = cluster.map_shared_rank(cta, c2);
+            const T pp = rc[2 * W + lane];
 #pragma unroll
             for (int r = 0; r < NR; r++) cin[r] = rc[r * W + lane] + pp * cin[r];
         }
     } else {
         for (int c2 = a.C - 1; c2 > crank; c2--) {
-            const double *rc = cluster.map_shared_rank(cta, c2);
-            const double pp = rc[5 * W + lane];
+            const T *rc = cluster.map_shared_rank(cta, c2);
+            const T pp = rc[5 * W + lane];
 #pragma unroll
             for (int r = 0; r < NR; r++) cin[r] = rc[(3 + r) * W + lane] + pp * cin[r];
         }
@@ -247,16 +260,25 @@ __device__ __forceinline__ void xl_inflow(const XFArgs &a, cg::cluster_group &cl
 
 // Exact split Thomas solve over the core rows of the tile(s), NR = 1 or 2
 // systems with the same matrix: operator OP0 on tile t0 and (NR = 2)
-// operator OP1 on tile t1.  Results go to global memory (column pointers
-// g0/g1, row stride ny) and/or, for one system, back into the tile's core
-// rows (tout).  `par` alternates between calls so that consecutive solves
-// exchange carries through different arrays; the caller issues a cluster
-// barrier before reading results of other CTAs.
-template <int W, int OP0, int OP1, int NR>
-__device__ void xl_solve(const XFArgs &a, const XLSmem &s, cg::cluster_group &cluster,
-                         const double *t0, const double *t1, double *g0, double *g1, double *tout,
-                         int Rc, long r0, int crank, int par)
+// operator OP1 on tile t1.  The right-hand sides are formed in FP64 from the
+// FP64 tiles; the recurrences run in T.  Results go to global memory (column
+// pointers g0/g1 of type OT, row stride ny) and/or, for one system, back
+// into the tile's core rows (tout).
+//   T = double: the reference's solves.
+//   T = float (mixed precision): derivatives are stored as floats; the
+//   filter is solved for its change d = A^-1 (B - A) u, the right-hand side
+//   (B - A) u formed in FP64, and u + d is accumulated in FP64.
+// `par` alternates between calls so that consecutive solves exchange carries
+// through different arrays; the caller issues a cluster barrier before
+// reading results of other CTAs.
+template <int W, int OP0, int OP1, int NR, typename T>
+__device__ void xl_solve(const XFArgs &a, const XLSmem<T> &s, cg::cluster_group &cluster,
+                         const double *t0, const double *t1,
+                         typename XLOut<OP0, T>::type *g0, typename XLOut<OP0, T>::type *g1,
+                         double *tout, int Rc, long r0, int crank, int par)
 {
+    using OT = typename XLOut<OP0, T>::type;
+    constexpr bool DELTA = OP0 == XOP_F && sizeof(T) == 4;  // filter change in FP32
     constexpr int NSUB = XLGeom<W>::NSUB;
     constexpr int MAT = OP0 == XOP_F ? 1 : 0;
     static_assert(NR == 1 || (OP1 != XOP_F && MAT == 0), "paired systems share the matrix");
@@ -266,15 +288,15 @@ __device__ void xl_solve(const XFArgs &a, const XLSmem &s, cg::cluster_group &cl
     const int la = sub * XL_S;
     // interior sub-chunk: constant factors, branch-free stencils, no row checks
     const bool fast = !((r0 + la < XF_EDGE) || (r0 + la + XL_S > nx - XF_EDGE)) && la + XL_S <= Rc;
-    const double m_in = a.tb.inner[MAT][0], ib_in = a.tb.inner[MAT][1], g_in = a.tb.inner[MAT][2];
-    double *cta = s.cta[par];
+    const T m_in = (T)a.tb.inner[MAT][0], ib_in = (T)a.tb.inner[MAT][1], g_in = (T)a.tb.inner[MAT][2];
+    T *cta = s.cta[par];
     const bool same = NR == 2 && t1 == t0;
-    double y[NR][XL_S];
+    T y[NR][XL_S];
 
     // ---- forward recurrence with zero inflow ------------------------------
-    double yv[NR], P = 1.0;
+    T yv[NR], P = (T)1;
 #pragma unroll
-    for (int r = 0; r < NR; r++) yv[r] = 0.0;
+    for (int r = 0; r < NR; r++) yv[r] = (T)0;
     if (fast) {
         const double *tw = t0 + (XL_H - 3) * W + lane;  // tw[r * W] = input of local row r - 3
         double w0 = tw[(la + 0) * W], w1 = tw[(la + 1) * W], w2 = tw[(la + 2) * W];
@@ -289,21 +311,23 @@ __device__ void xl_solve(const XFArgs &a, const XLSmem &s, cg::cluster_group &cl
         for (int k = 0; k < XL_S; k++) {
             const int l = la + k;
             const double w6 = tw[(l + 6) * W];
-            yv[0] = xl_rhs<OP0>(a.st[OP0], w0, w1, w2, w3, w4, w5, w6) - m_in * yv[0];
+            double rhs = xl_rhs<OP0>(a.st[OP0], w0, w1, w2, w3, w4, w5, w6);
+            if constexpr (DELTA) rhs -= a.fa_in * (w2 + w4) + w3;  // (B - A) u
+            yv[0] = (T)rhs - m_in * yv[0];
             y[0][k] = yv[0];
             if constexpr (NR == 2) {
                 if (same) {
-                    yv[1] = xl_rhs<OP1>(a.st[OP1], w0, w1, w2, w3, w4, w5, w6) - m_in * yv[1];
+                    yv[1] = (T)xl_rhs<OP1>(a.st[OP1], w0, w1, w2, w3, w4, w5, w6) - m_in * yv[1];
                 } else {
                     const double v6 = tv[(l + 6) * W];
-                    yv[1] = xl_rhs<OP1>(a.st[OP1], v0, v1, v2, v3, v4, v5, v6) - m_in * yv[1];
+                    yv[1] = (T)xl_rhs<OP1>(a.st[OP1], v0, v1, v2, v3, v4, v5, v6) - m_in * yv[1];
                     v0 = v1; v1 = v2; v2 = v3; v3 = v4; v4 = v5; v5 = v6;
                 }
                 y[NR - 1][k] = yv[NR - 1];
             }
             w0 = w1; w1 = w2; w2 = w3; w3 = w4; w4 = w5; w5 = w6;
         }
-        P = a.pw[MAT][0];  // (-m)^XL_S, formed on the host as the rows would form it
+        P = (T)a.pw[MAT][0];  // (-m)^XL_S, formed on the host as the rows would form it
     } else {  // near a line end or past the last row: tabulated factors, closures
 #pragma unroll
         for (int r = 0; r < NR; r++) {
@@ -311,7 +335,7 @@ __device__ void xl_solve(const XFArgs &a, const XLSmem &s, cg::cluster_group &cl
             double w0 = tw[(la + 0) * W], w1 = tw[(la + 1) * W], w2 = tw[(la + 2) * W];
             double w3 = tw[(la + 3) * W], w4 = tw[(la + 4) * W], w5 = tw[(la + 5) * W];
             const XStencil &st = a.st[r == 0 ? OP0 : OP1];
-            double pp = 1.0;
+            T pp = (T)1;
 #pragma unroll
             for (int k = 0; k < XL_S; k++) {
                 const int l = la + k;
@@ -319,8 +343,13 @@ __device__ void xl_solve(const XFArgs &a, const XLSmem &s, cg::cluster_group &cl
                 double w6 = tw[(l + 6) * W];
                 if (l < Rc) {
                     double rhs = stencil(st, w0, w1, w2, w3, w4, w5, w6, gr, nx);
-                    double m = xl_tab(s.tab, a.tb, MAT, 0, gr, nx);
-                    yv[r] = rhs - m * yv[r];
+                    if constexpr (DELTA) {  // (B - A) u with the matrix rows of initTriMatrix
+                        const double lo = gr == 0 ? 0.0 : (gr == nx - 1 ? a.fa_sub : a.fa_in);
+                        const double up = gr == nx - 1 ? 0.0 : (gr == 0 ? a.fa_sub : a.fa_in);
+                        rhs -= lo * w2 + w3 + up * w4;
+                    }
+                    T m = (T)xl_tab(s.tab, a.tb, MAT, 0, gr, nx);
+                    yv[r] = (T)rhs - m * yv[r];
                     pp *= -m;
                 }
                 y[r][k] = yv[r];
@@ -333,48 +362,48 @@ __device__ void xl_solve(const XFArgs &a, const XLSmem &s, cg::cluster_group &cl
     for (int r = 0; r < NR; r++) s.aggE[r][ai] = yv[r];
     s.aggP[ai] = P;
     __syncthreads();
-    xl_scan<W, NR>(s, cta, 0, false);
+    xl_scan<W, NR, T>(s, cta, 0, false);
     cluster.sync();
 
     // ---- forward inflow and fix-up; backward recurrence with zero inflow --
-    double cin[NR];
-    xl_inflow<W, NR>(a, cluster, cta, crank, 0, lane, cin);
-    double xv[NR], Q = 1.0;
+    T cin[NR];
+    xl_inflow<W, NR, T>(a, cluster, cta, crank, 0, lane, cin);
+    T xv[NR], Q = (T)1;
     {
-        const double pP = s.preP[ai];
+        const T pP = s.preP[ai];
 #pragma unroll
         for (int r = 0; r < NR; r++) {
-            double d = s.preE[r][ai] + pP * cin[r];
+            T d = s.preE[r][ai] + pP * cin[r];
             if (fast) {
 #pragma unroll
                 for (int k = 0; k < XL_S; k++) {
                     d *= -m_in;
                     y[r][k] += d;
                 }
-                double x = 0.0;
+                T x = (T)0;
 #pragma unroll
                 for (int k = XL_S - 1; k >= 0; k--) {
                     x = y[r][k] * ib_in - g_in * x;
                     y[r][k] = x;
                 }
                 xv[r] = x;
-                Q = a.pw[MAT][1];  // (-g)^XL_S
+                Q = (T)a.pw[MAT][1];  // (-g)^XL_S
             } else {
 #pragma unroll
                 for (int k = 0; k < XL_S; k++) {
                     const int l = la + k;
                     if (l < Rc) {
-                        d *= -xl_tab(s.tab, a.tb, MAT, 0, r0 + l, nx);
+                        d *= -(T)xl_tab(s.tab, a.tb, MAT, 0, r0 + l, nx);
                         y[r][k] += d;
                     }
                 }
-                double x = 0.0, qq = 1.0;
+                T x = (T)0, qq = (T)1;
 #pragma unroll
                 for (int k = XL_S - 1; k >= 0; k--) {
                     const int l = la + k;
                     if (l < Rc) {
-                        double g = xl_tab(s.tab, a.tb, MAT, 2, r0 + l, nx);
-                        x = y[r][k] * xl_tab(s.tab, a.tb, MAT, 1, r0 + l, nx) - g * x;
+                        T g = (T)xl_tab(s.tab, a.tb, MAT, 2, r0 + l, nx);
+                        x = y[r][k] * (T)xl_tab(s.tab, a.tb, MAT, 1, r0 + l, nx) - g * x;
                         qq *= -g;
                         y[r][k] = x;
                     }
@@ -389,26 +418,31 @@ __device__ void xl_solve(const XFArgs &a, const XLSmem &s, cg::cluster_group &cl
     for (int r = 0; r < NR; r++) s.aggE[r][ai] = xv[r];
     s.aggP[ai] = Q;
     __syncthreads();
-    xl_scan<W, NR>(s, cta, 3, true);
+    xl_scan<W, NR, T>(s, cta, 3, true);
     cluster.sync();
 
     // ---- backward inflow, fix-up and results -------------------------------
-    double cb[NR];
-    xl_inflow<W, NR>(a, cluster, cta, crank, 1, lane, cb);
-    const double pQ = s.preP[ai];
+    T cb[NR];
+    xl_inflow<W, NR, T>(a, cluster, cta, crank, 1, lane, cb);
+    const T pQ = s.preP[ai];
 #pragma unroll
     for (int r = 0; r < NR; r++) {
-        double d = s.preE[r][ai] + pQ * cb[r];
-        double *g = r == 0 ? g0 : g1;
+        T d = s.preE[r][ai] + pQ * cb[r];
+        OT *g = r == 0 ? g0 : g1;
         if (g) g += (size_t)r0 * ny;
 #pragma unroll
         for (int k = XL_S - 1; k >= 0; k--) {
             const int l = la + k;
             if (l < Rc) {
-                d *= fast ? -g_in : -xl_tab(s.tab, a.tb, MAT, 2, r0 + l, nx);
-                double v = y[r][k] + d;
+                d *= fast ? -g_in : -(T)xl_tab(s.tab, a.tb, MAT, 2, r0 + l, nx);
+                const T x = y[r][k] + d;
+                OT v;
+                if constexpr (DELTA) v = t0[(l + XL_H) * W + lane] + (double)x;  // u + d in FP64
+                else v = (OT)x;
                 if (g) g[(size_t)l * ny] = v;
-                if (NR == 1 && tout) tout[(l + XL_H) * W + lane] = v;
+                if constexpr (NR == 1 && OP0 == XOP_F) {
+                    if (tout) tout[(l + XL_H) * W + lane] = (double)v;
+                }
             }
         }
     }
@@ -443,8 +477,8 @@ __device__ __forceinline__ int xl_runs(long r0, int Rc, long nx, XLRun run[3])
 }
 
 // Issue the TMA copies of field `v` into tile buffer `b`; warp 0 only.
-template <int W>
-__device__ __forceinline__ void xl_stage(const XFArgs &a, const XLSmem &s, int b, int v, long r0,
+template <int W, typename T>
+__device__ __forceinline__ void xl_stage(const XFArgs &a, const XLSmem<T> &s, int b, int v, long r0,
                                          int Rc, long j0, const CUtensorMap *big,
                                          const CUtensorMap *unit)
 {
@@ -492,8 +526,8 @@ __device__ __forceinline__ void xl_stage(const XFArgs &a, const XLSmem &s, int b
     }
 }
 
-template <int W>
-__global__ void __launch_bounds__(XL_T, 1)
+template <int W, typename T>
+__global__ void __launch_bounds__(XL_T, MHD_XLINE_MINB)
 xline_kernel(XFArgs a, const __grid_constant__ CUtensorMap tm_big,
              const __grid_constant__ CUtensorMap tm_unit)
 {
@@ -510,7 +544,10 @@ xline_kernel(XFArgs a, const __grid_constant__ CUtensorMap tm_big,
     const size_t plane = (size_t)nx * ny;
     const int tid = threadIdx.x, lane = tid % W;
     const bool col = lane < ncols;
-    XLSmem s = xl_carve<W>(xl_raw);
+    XLSmem<T> s = xl_carve<W, T>(xl_raw);
+    T *const o1 = reinterpret_cast<T *>(a.out1);  // derivative outputs hold T
+    T *const o2a = reinterpret_cast<T *>(a.out2a), *const o2b = reinterpret_cast<T *>(a.out2b);
+    T *const oE = reinterpret_cast<T *>(a.outE);
 
     for (int i = tid; i < 2 * 3 * 2 * XF_EDGE; i += XL_T) s.tab[i] = a.tb.edge[i];
     if (tid == 0) {
@@ -535,19 +572,22 @@ xline_kernel(XFArgs a, const __grid_constant__ CUtensorMap tm_big,
         __syncthreads();
         double *t = s.tile[b];
         if (a.single_op >= 0) {  // one operator per field
-            double *g = (a.out1 && col) ? a.out1 + (size_t)f * plane + j0 + lane : nullptr;
-            if (a.single_op == XOP_F)
-                xl_solve<W, XOP_F, XOP_F, 1>(a, s, cluster, t, t, g, nullptr, nullptr, Rc, r0, crank, par);
+            const size_t off = (size_t)f * plane + j0 + lane;
+            if (a.single_op == XOP_F)  // the filter writes FP64 state
+                xl_solve<W, XOP_F, XOP_F, 1, T>(a, s, cluster, t, t, (a.out1 && col) ? a.out1 + off : nullptr,
+                                                nullptr, nullptr, Rc, r0, crank, par);
             else if (a.single_op == XOP_D1)
-                xl_solve<W, XOP_D1, XOP_D1, 1>(a, s, cluster, t, t, g, nullptr, nullptr, Rc, r0, crank, par);
+                xl_solve<W, XOP_D1, XOP_D1, 1, T>(a, s, cluster, t, t, (o1 && col) ? o1 + off : nullptr,
+                                                  nullptr, nullptr, Rc, r0, crank, par);
             else
-                xl_solve<W, XOP_D2, XOP_D2, 1>(a, s, cluster, t, t, g, nullptr, nullptr, Rc, r0, crank, par);
+                xl_solve<W, XOP_D2, XOP_D2, 1, T>(a, s, cluster, t, t, (o1 && col) ? o1 + off : nullptr,
+                                                  nullptr, nullptr, Rc, r0, crank, par);
             par ^= 1;
             continue;
         }
         if (a.fout) {
             double *g = col ? a.fout + (size_t)v * plane + j0 + lane : nullptr;
-            xl_solve<W, XOP_F, XOP_F, 1>(a, s, cluster, t, t, g, nullptr, t, Rc, r0, crank, par);
+            xl_solve<W, XOP_F, XOP_F, 1, T>(a, s, cluster, t, t, g, nullptr, t, Rc, r0, crank, par);
             par ^= 1;
             cluster.sync();  // every CTA's tile holds its filtered core rows
             // halo rows of the filtered line from the neighbouring CTAs
@@ -565,17 +605,18 @@ xline_kernel(XFArgs a, const __grid_constant__ CUtensorMap tm_big,
             __syncthreads();
         }
         if (!a.out1) continue;
-        double *g1 = col ? a.out1 + (size_t)v * plane + j0 + lane : nullptr;
-        double *g2 = nullptr;
-        if (a.out2a && v >= a.d2a_lo && v < a.d2a_lo + 3)
-            g2 = a.out2a + (size_t)(v - a.d2a_lo) * plane + j0 + lane;
-        else if (a.out2b && v >= a.d2b_lo && v < a.d2b_lo + 3)
-            g2 = a.out2b + (size_t)(v - a.d2b_lo) * plane + j0 + lane;
+        T *g1 = col ? o1 + (size_t)v * plane + j0 + lane : nullptr;
+        T *g2 = nullptr;
+        if (o2a && v >= a.d2a_lo && v < a.d2a_lo + 3)
+            g2 = o2a + (size_t)(v - a.d2a_lo) * plane + j0 + lane;
+        else if (o2b && v >= a.d2b_lo && v < a.d2b_lo + 3)
+            g2 = o2b + (size_t)(v - a.d2b_lo) * plane + j0 + lane;
         if (g2)  // d/dx and d2/dx2 share the matrix: one paired solve
-            xl_solve<W, XOP_D1, XOP_D2, 2>(a, s, cluster, t, t, g1, col ? g2 : nullptr, nullptr, Rc,
-                                           r0, crank, par);
+            xl_solve<W, XOP_D1, XOP_D2, 2, T>(a, s, cluster, t, t, g1, col ? g2 : nullptr, nullptr, Rc,
+                                              r0, crank, par);
         else
-            xl_solve<W, XOP_D1, XOP_D1, 1>(a, s, cluster, t, t, g1, nullptr, nullptr, Rc, r0, crank, par);
+            xl_solve<W, XOP_D1, XOP_D1, 1, T>(a, s, cluster, t, t, g1, nullptr, nullptr, Rc, r0, crank,
+                                              par);
         par ^= 1;
     }
 
@@ -599,10 +640,10 @@ xline_kernel(XFArgs a, const __grid_constant__ CUtensorMap tm_big,
         }
         __syncthreads();
         // Ey and Ez share the matrix: one paired solve
-        xl_solve<W, XOP_D1, XOP_D1, 2>(a, s, cluster, s.tile[0], s.tile[1],
-                                       col ? a.outE + j0 + lane : nullptr,
-                                       col ? a.outE + plane + j0 + lane : nullptr, nullptr, Rc, r0,
-                                       crank, par);
+        xl_solve<W, XOP_D1, XOP_D1, 2, T>(a, s, cluster, s.tile[0], s.tile[1],
+                                          col ? oE + j0 + lane : nullptr,
+                                          col ? oE + plane + j0 + lane : nullptr, nullptr, Rc, r0,
+                                          crank, par);
         par ^= 1;
     }
     cluster.sync();  // peers may still read this CTA's shared memory
@@ -676,6 +717,23 @@ static int xl_tensor_map(CUtensorMap *map, const double *base, long rows, long n
 static long xl_rcap(int W)
 {
     return W == 32 ? XLGeom<32>::RCAP : W == 16 ? XLGeom<16>::RCAP : XLGeom<8>::RCAP;
+}
+
+template <typename T>
+static int xl_attrs(int C)
+{
+    MHD_CUDA_TRY(cudaFuncSetAttribute(xline_kernel<32, T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)xl_smem_bytes<32>()));
+    MHD_CUDA_TRY(cudaFuncSetAttribute(xline_kernel<16, T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)xl_smem_bytes<16>()));
+    MHD_CUDA_TRY(cudaFuncSetAttribute(xline_kernel<8, T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)xl_smem_bytes<8>()));
+    if (C > 8) {
+        MHD_CUDA_TRY(cudaFuncSetAttribute(xline_kernel<32, T>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
+        MHD_CUDA_TRY(cudaFuncSetAttribute(xline_kernel<16, T>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
+        MHD_CUDA_TRY(cudaFuncSetAttribute(xline_kernel<8, T>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
+    }
+    return MHDGPU_OK;
 }
 
 int xline_setup(Ctx *c)
@@ -766,17 +824,8 @@ int xline_setup(Ctx *c)
     if ((rc = xl_tensor_map(&c->xl_tmap_big, c->arr[MHDGPU_UU], rows, c->ny, W, XL_BOX))) return rc;
     if ((rc = xl_tensor_map(&c->xl_tmap_unit, c->arr[MHDGPU_UU], rows, c->ny, W, W == 8 ? 2 : 1)))
         return rc;
-    MHD_CUDA_TRY(cudaFuncSetAttribute(xline_kernel<32>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      (int)xl_smem_bytes<32>()));
-    MHD_CUDA_TRY(cudaFuncSetAttribute(xline_kernel<16>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      (int)xl_smem_bytes<16>()));
-    MHD_CUDA_TRY(cudaFuncSetAttribute(xline_kernel<8>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      (int)xl_smem_bytes<8>()));
-    if (C > 8) {
-        MHD_CUDA_TRY(cudaFuncSetAttribute(xline_kernel<32>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
-        MHD_CUDA_TRY(cudaFuncSetAttribute(xline_kernel<16>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
-        MHD_CUDA_TRY(cudaFuncSetAttribute(xline_kernel<8>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
-    }
+    if ((rc = xl_attrs<double>(C))) return rc;
+    if ((rc = xl_attrs<float>(C))) return rc;
     return MHDGPU_OK;
 }
 
@@ -798,6 +847,8 @@ int launch_xline(Ctx *c, const XFArgs &proto, double bytes)
     a.R = c->xf_R;
     a.C = c->xf_C;
     a.hops = c->xf_hops;
+    a.fa_in = c->xf_alphaF[0];
+    a.fa_sub = c->xf_alphaF[1];
     std::memcpy(a.pw, c->xf_pw, sizeof a.pw);
     a.flag = c->dflag;
     const int W = c->xf_W;
@@ -814,15 +865,26 @@ int launch_xline(Ctx *c, const XFArgs &proto, double bytes)
     cfg.attrs = attr;
     cfg.numAttrs = 1;
     prof_begin(c, KC_FUSED_X, bytes);
-    if (W == 32) {
+    if (c->mixed) {
+        if (W == 32) {
+            cfg.dynamicSmemBytes = xl_smem_bytes<32>();
+            MHD_CUDA_TRY(cudaLaunchKernelEx(&cfg, xline_kernel<32, float>, a, c->xl_tmap_big, c->xl_tmap_unit));
+        } else if (W == 16) {
+            cfg.dynamicSmemBytes = xl_smem_bytes<16>();
+            MHD_CUDA_TRY(cudaLaunchKernelEx(&cfg, xline_kernel<16, float>, a, c->xl_tmap_big, c->xl_tmap_unit));
+        } else {
+            cfg.dynamicSmemBytes = xl_smem_bytes<8>();
+            MHD_CUDA_TRY(cudaLaunchKernelEx(&cfg, xline_kernel<8, float>, a, c->xl_tmap_big, c->xl_tmap_unit));
+        }
+    } else if (W == 32) {
         cfg.dynamicSmemBytes = xl_smem_bytes<32>();
-        MHD_CUDA_TRY(cudaLaunchKernelEx(&cfg, xline_kernel<32>, a, c->xl_tmap_big, c->xl_tmap_unit));
+        MHD_CUDA_TRY(cudaLaunchKernelEx(&cfg, xline_kernel<32, double>, a, c->xl_tmap_big, c->xl_tmap_unit));
     } else if (W == 16) {
         cfg.dynamicSmemBytes = xl_smem_bytes<16>();
-        MHD_CUDA_TRY(cudaLaunchKernelEx(&cfg, xline_kernel<16>, a, c->xl_tmap_big, c->xl_tmap_unit));
+        MHD_CUDA_TRY(cudaLaunchKernelEx(&cfg, xline_kernel<16, double>, a, c->xl_tmap_big, c->xl_tmap_unit));
     } else {
         cfg.dynamicSmemBytes = xl_smem_bytes<8>();
-        MHD_CUDA_TRY(cudaLaunchKernelEx(&cfg, xline_kernel<8>, a, c->xl_tmap_big, c->xl_tmap_unit));
+        MHD_CUDA_TRY(cudaLaunchKernelEx(&cfg, xline_kernel<8, double>, a, c->xl_tmap_big, c->xl_tmap_unit));
     }
     prof_end(c);
     return MHDGPU_OK;

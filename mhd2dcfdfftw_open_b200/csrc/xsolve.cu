@@ -269,6 +269,8 @@ int xsolve_setup(Ctx *c)
     const long n = c->nx;
     double alpha[3][2];
     scheme_constants(c->dx, c->xs, alpha);
+    c->xf_alphaF[0] = alpha[XOP_F][0];
+    c->xf_alphaF[1] = alpha[XOP_F][1];
     for (int op = 0; op < 3; op++) {
         // initTriMatrixCFD* for a periodic boundary (initialize.c:636-654):
         // lower[i] (row i+1) = alpha_inner except lower[n-2] = alpha_sub,

@@ -25,9 +25,12 @@ constexpr int YR_THREADS = 256;
 
 struct YRArgs {
     double *uu, *dudtRK;
-    const double *dudx, *d2udx2, *d2Bdx2, *dEdx;
-    double *dudy, *d2udy2, *d2Bdy2, *dEdy;
+    // derivative arrays: doubles, or floats (field v at v * nx * ny) in the
+    // mixed-precision stage
+    const void *dudx, *d2udx2, *d2Bdx2, *dEdx;
+    void *dudy, *d2udy2, *d2Bdy2, *dEdy;
     const double2 *tw, *s1, *s2, *sf;  // twiddles; symbols of d/dy, d2/dy2, filter
+    const float2 *tw32, *s1_32, *s2_32, *sfd32;  // float twiddles, symbols, filter - identity
     long nx, ny;
     int nvar;
     RhsCoef k;
@@ -37,83 +40,110 @@ struct YRArgs {
     int *flag;     // status flag of bounded waits
 };
 
-template <int L>
+template <typename T> struct YRCplx;
+template <> struct YRCplx<double> { using C = double2; };
+template <> struct YRCplx<float> { using C = float2; };
+
+template <int L, typename T>
 struct YRGeom {
+    using C = typename YRCplx<T>::C;
     static constexpr int N = 1 << L;
-    static constexpr int T = N / 16;                                  // threads per row
-    static constexpr int ROWS = T >= YR_THREADS ? 1 : YR_THREADS / T;  // rows per CTA
-    static constexpr int NP = N + N / 16;                             // padded row
-    // shared memory: one padded FFT row per row of the CTA (68 KB for any
-    // row length), so that two CTAs share an SM
-    static constexpr size_t SMEM = sizeof(double2) * ROWS * NP;
+    static constexpr int T_ = N / 16;                                   // threads per row
+    static constexpr int ROWS = T_ >= YR_THREADS ? 1 : YR_THREADS / T_;  // rows per CTA
+    static constexpr int NP = N + N / 16;                              // padded row
+    // shared memory: one padded FFT row per row of the CTA (68 KB in FP64,
+    // 34 KB in FP32, for any row length)
+    static constexpr size_t SMEM = sizeof(C) * ROWS * NP;
+    // CTAs per SM the register budget is set for
+    static constexpr int MINB = sizeof(T) == 8 ? 2 : 3;
 };
 
 // Load fields fa and fb (fb < 0: zero) of this group's row into the FFT row
-// as fa + i fb; each thread its own 16 points, coalesced across the group.
-template <int L>
-__device__ __forceinline__ void yr_load(double2 *A, const double *ra, const double *rb, int j,
-                                        bool valid)
+// as (fa - ca) + i (fb - cb); each thread its own 16 points, coalesced across
+// the group.  ca/cb are 0 in FP64; in FP32 they are the row's first values,
+// subtracted in FP64: the operators applied here (d/dy, d2/dy2 and filter
+// minus identity) map constants to zero, and the FP32 row then carries only
+// the variation along the row.
+template <int L, typename T>
+__device__ __forceinline__ void yr_load(typename YRCplx<T>::C *A, const double *ra,
+                                        const double *rb, double ca, double cb, int j, bool valid)
 {
-    using G = YRGeom<L>;
+    using G = YRGeom<L, T>;
     double va[16], vb[16];
 #pragma unroll
     for (int m = 0; m < 16; m++) {
-        const int i = j + m * G::T;
+        const int i = j + m * G::T_;
         va[m] = valid ? ra[i] : 0.0;
         vb[m] = (valid && rb) ? rb[i] : 0.0;
     }
 #pragma unroll
-    for (int m = 0; m < 16; m++) A[fpad(j + m * G::T)] = make_double2(va[m], vb[m]);
+    for (int m = 0; m < 16; m++)
+        A[fpad(j + m * G::T_)] = cmk<typename G::C>((T)(va[m] - ca), (T)(vb[m] - cb));
 }
 
 // One spectral operator on the row in A (natural order, already loaded):
-// forward FFT, multiply by the symbol s, inverse FFT, real part to oa and
-// imaginary part to ob (null: skipped).  Ends with the block synchronised.
-template <int L>
-__device__ __forceinline__ void yr_op(const YRArgs &a, double2 *A, int j, bool valid,
-                                      const double2 *s, double *oa, double *ob)
+// forward FFT, multiply by the symbol s, inverse FFT; the real part goes to
+// oa and the imaginary part to ob (null: skipped), stored as T, or with ACC
+// added to the doubles there.  Ends with the block synchronised.
+template <int L, typename T, bool ACC, typename O>
+__device__ __forceinline__ void yr_op(const typename YRCplx<T>::C *tw, typename YRCplx<T>::C *A,
+                                      int j, bool valid, const typename YRCplx<T>::C *s, O *oa,
+                                      O *ob)
 {
-    using G = YRGeom<L>;
+    using G = YRGeom<L, T>;
     __syncthreads();  // the row is complete
-    fft_row<L, -1>(A, a.tw, j);
+    fft_row<L, -1>(A, tw, j);
 #pragma unroll
     for (int m = 0; m < 16; m++) {
-        const int i = j + m * G::T;
+        const int i = j + m * G::T_;
         A[fpad(i)] = cm(A[fpad(i)], __ldg(s + i));
     }
     __syncthreads();
-    fft_row<L, +1>(A, a.tw, j);
+    fft_row<L, +1>(A, tw, j);
     if (valid) {
 #pragma unroll
         for (int m = 0; m < 16; m++) {
-            const int i = j + m * G::T;
-            double2 z = A[fpad(i)];
-            if (oa) oa[i] = z.x;
-            if (ob) ob[i] = z.y;
+            const int i = j + m * G::T_;
+            const typename G::C z = A[fpad(i)];
+            if constexpr (ACC) {
+                if (oa) oa[i] += (double)z.x;
+                if (ob) ob[i] += (double)z.y;
+            } else {
+                if (oa) oa[i] = (O)z.x;
+                if (ob) ob[i] = (O)z.y;
+            }
         }
     }
     __syncthreads();  // A may be refilled
 }
 
-template <int L>
-__global__ void __launch_bounds__(YR_THREADS, 2) yrow_kernel(YRArgs a)
+template <int L, typename T>
+__global__ void __launch_bounds__(YR_THREADS, (YRGeom<L, T>::MINB)) yrow_kernel(YRArgs a)
 {
-    using G = YRGeom<L>;
+    using G = YRGeom<L, T>;
+    using C = typename G::C;
+    constexpr bool MIX = sizeof(T) == 4;
     extern __shared__ __align__(128) unsigned char yr_raw[];
-    double2 *Abase = reinterpret_cast<double2 *>(yr_raw);
-    const int g = threadIdx.x / G::T, j = threadIdx.x % G::T;
+    C *Abase = reinterpret_cast<C *>(yr_raw);
+    const int g = threadIdx.x / G::T_, j = threadIdx.x % G::T_;
     const long row = (long)blockIdx.x * G::ROWS + g;
     const bool valid = row < a.nx;
-    double2 *A = Abase + (size_t)g * G::NP;
+    C *A = Abase + (size_t)g * G::NP;
     const size_t plane = (size_t)a.nx * a.ny;
     const size_t ro = valid ? (size_t)row * a.ny : 0;
-    // row `ro` of field v of array base (null base: null)
-    auto f = [&](double *base, int v) -> double * {
-        return base ? base + (size_t)v * plane + ro : nullptr;
+    const C *tw = MIX ? reinterpret_cast<const C *>(a.tw32) : reinterpret_cast<const C *>(a.tw);
+    const C *s1 = MIX ? reinterpret_cast<const C *>(a.s1_32) : reinterpret_cast<const C *>(a.s1);
+    const C *s2 = MIX ? reinterpret_cast<const C *>(a.s2_32) : reinterpret_cast<const C *>(a.s2);
+    // row `ro` of field v of a derivative array of T (null base: null)
+    auto f = [&](void *base, int v) -> T * {
+        return base ? reinterpret_cast<T *>(base) + (size_t)v * plane + ro : nullptr;
     };
-    auto fc = [&](const double *base, int v) -> const double * {
-        return base ? base + (size_t)v * plane + ro : nullptr;
+    auto fc = [&](const void *base, int v) -> const T * {
+        return base ? reinterpret_cast<const T *>(base) + (size_t)v * plane + ro : nullptr;
     };
+    auto su = [&](int v) -> double * { return a.uu + (size_t)v * plane + ro; };
+    // the row shift of the FP32 operators (see yr_load)
+    auto sh = [&](const double *r) -> double { return MIX && valid ? r[0] : 0.0; };
 
     // ---- 1. y-derivatives: pairs (ux,uy) (rho,p) (uz,Bz) (Bx,By) [psi],
     // d/dy of every field, d2/dy2 of u and B (a second forward FFT of the
@@ -122,9 +152,11 @@ __global__ void __launch_bounds__(YR_THREADS, 2) yrow_kernel(YRArgs a)
     for (int q = 0; q < npair; q++) {
         const int fa = q == 0 ? UX : q == 1 ? RHO : q == 2 ? UZ : q == 3 ? BX : PSI;
         const int fb = q == 0 ? UY : q == 1 ? P : q == 2 ? BZ : q == 3 ? BY : -1;
-        yr_load<L>(A, fc(a.uu, fa), fb >= 0 ? fc(a.uu, fb) : nullptr, j, valid);
-        yr_op<L>(a, A, j, valid, a.s1, f(a.dudy, fa), fb >= 0 ? f(a.dudy, fb) : nullptr);
-        double *o2a = nullptr, *o2b = nullptr;
+        const double *ra = su(fa), *rb = fb >= 0 ? su(fb) : nullptr;
+        const double ca = sh(ra), cb = rb ? sh(rb) : 0.0;
+        yr_load<L, T>(A, ra, rb, ca, cb, j, valid);
+        yr_op<L, T, false>(tw, A, j, valid, s1, f(a.dudy, fa), fb >= 0 ? f(a.dudy, fb) : nullptr);
+        T *o2a = nullptr, *o2b = nullptr;
         if (fa == UX && a.d2u) { o2a = f(a.d2udy2, 0); o2b = f(a.d2udy2, 1); }
         if (fa == UZ) {
             o2a = a.d2u ? f(a.d2udy2, 2) : nullptr;
@@ -132,58 +164,75 @@ __global__ void __launch_bounds__(YR_THREADS, 2) yrow_kernel(YRArgs a)
         }
         if (fa == BX && a.d2b) { o2a = f(a.d2Bdy2, 0); o2b = f(a.d2Bdy2, 1); }
         if (o2a || o2b) {  // uniform across the block
-            yr_load<L>(A, fc(a.uu, fa), fc(a.uu, fb), j, valid);
-            yr_op<L>(a, A, j, valid, a.s2, o2a, o2b);
+            yr_load<L, T>(A, ra, rb, ca, cb, j, valid);
+            yr_op<L, T, false>(tw, A, j, valid, s2, o2a, o2b);
         }
     }
-    {   // (Ex, Ez) = (uz By - uy Bz, uy Bx - ux By)
+    {   // (Ex, Ez) = (uz By - uy Bz, uy Bx - ux By), formed in FP64
+        auto efield = [&](size_t o, double &ex, double &ez) {
+            const double *u = a.uu + o;
+            double ux = u[UX * plane], uy = u[UY * plane], uz = u[UZ * plane];
+            double bx = u[BX * plane], by = u[BY * plane], bz = u[BZ * plane];
+            ex = uz * by - uy * bz;
+            ez = uy * bx - ux * by;
+        };
+        double cx = 0.0, cz = 0.0;
+        if (MIX && valid) efield(ro, cx, cz);
 #pragma unroll 4
         for (int m = 0; m < 16; m++) {
-            const int i = j + m * G::T;
-            double2 z = make_double2(0.0, 0.0);
-            if (valid) {
-                const double *u = a.uu + ro + i;
-                double ux = u[UX * plane], uy = u[UY * plane], uz = u[UZ * plane];
-                double bx = u[BX * plane], by = u[BY * plane], bz = u[BZ * plane];
-                z = make_double2(uz * by - uy * bz, uy * bx - ux * by);
-            }
-            A[fpad(i)] = z;
+            const int i = j + m * G::T_;
+            double ex = 0.0, ez = 0.0;
+            if (valid) efield(ro + i, ex, ez);
+            A[fpad(i)] = cmk<C>((T)(ex - cx), (T)(ez - cz));
         }
-        yr_op<L>(a, A, j, valid, a.s1, f(a.dEdy, 0), f(a.dEdy, 2));
+        yr_op<L, T, false>(tw, A, j, valid, s1, f(a.dEdy, 0), f(a.dEdy, 2));
     }
 
     // ---- 2. right-hand side and RK3 update, point by point ------------------
+    // (FP64 state and RK3 accumulation in both precisions; the fluxes in T)
     if (valid) {
         const int nv = a.nvar;
+        const T *dEdx = reinterpret_cast<const T *>(a.dEdx);
+        const T *dEdy = reinterpret_cast<const T *>(a.dEdy);
+        const T *dudx = reinterpret_cast<const T *>(a.dudx);
+        const T *dudy = reinterpret_cast<const T *>(a.dudy);
+        const T *d2udx2 = reinterpret_cast<const T *>(a.d2udx2);
+        const T *d2udy2 = reinterpret_cast<const T *>(a.d2udy2);
+        const T *d2Bdx2 = reinterpret_cast<const T *>(a.d2Bdx2);
+        const T *d2Bdy2 = reinterpret_cast<const T *>(a.d2Bdy2);
 #pragma unroll 1
         for (int m = 0; m < 16; m++) {
-            const size_t o = ro + j + m * G::T;
-            double u[9], dx[9], dy[9], d2x[6], d2y[6], r[9];
+            const size_t o = ro + j + m * G::T_;
+            T u[9], dx[9], dy[9], d2x[6], d2y[6], r[9];
+            double ud[9];
 #pragma unroll
             for (int v = 0; v < 9; v++) {
                 if (v < nv) {
-                    u[v] = a.uu[v * plane + o];
-                    dx[v] = a.dudx[v * plane + o];
-                    dy[v] = a.dudy[v * plane + o];
+                    ud[v] = a.uu[v * plane + o];
+                    u[v] = (T)ud[v];
+                    dx[v] = dudx[v * plane + o];
+                    dy[v] = dudy[v * plane + o];
                 } else {
-                    u[v] = dx[v] = dy[v] = 0.0;
+                    ud[v] = 0.0;
+                    u[v] = dx[v] = dy[v] = (T)0;
                 }
             }
 #pragma unroll
             for (int c = 0; c < 3; c++) {
-                d2x[c] = a.k.visc > 0 ? a.d2udx2[c * plane + o] : 0.0;
-                d2y[c] = a.k.visc > 0 ? a.d2udy2[c * plane + o] : 0.0;
-                d2x[3 + c] = a.k.resist > 0 ? a.d2Bdx2[c * plane + o] : 0.0;
-                d2y[3 + c] = a.k.resist > 0 ? a.d2Bdy2[c * plane + o] : 0.0;
+                d2x[c] = a.k.visc > 0 ? d2udx2[c * plane + o] : (T)0;
+                d2y[c] = a.k.visc > 0 ? d2udy2[c * plane + o] : (T)0;
+                d2x[3 + c] = a.k.resist > 0 ? d2Bdx2[c * plane + o] : (T)0;
+                d2y[3 + c] = a.k.resist > 0 ? d2Bdy2[c * plane + o] : (T)0;
             }
-            rhs_point(a.k, u, dx, dy, d2x, d2y, a.dEdx[plane + o], a.dEdx[2 * plane + o],
-                      a.dEdy[o], a.dEdy[2 * plane + o], 0.0, 0.0, r);
+            rhs_point<T>(a.k, u, dx, dy, d2x, d2y, dEdx[plane + o], dEdx[2 * plane + o], dEdy[o],
+                         dEdy[2 * plane + o], (T)0, (T)0, r);
 #pragma unroll
             for (int v = 0; v < 9; v++) {
                 if (v < nv) {
                     double rk = a.read_rk ? a.dudtRK[v * plane + o] : 0.0;
-                    a.uu[v * plane + o] = u[v] + a.cc * r[v] + a.dd * rk;
-                    if (a.write_rk) a.dudtRK[v * plane + o] = r[v];
+                    const double rv = (double)r[v];
+                    a.uu[v * plane + o] = ud[v] + a.cc * rv + a.dd * rk;
+                    if (a.write_rk) a.dudtRK[v * plane + o] = rv;
                 }
             }
         }
@@ -191,31 +240,39 @@ __global__ void __launch_bounds__(YR_THREADS, 2) yrow_kernel(YRArgs a)
     __syncthreads();  // the updated rows are visible to the whole block
 
     // ---- 3. spectral y filter of the updated fields, two at a time ----------
+    // FP64: the filtered row replaces the row.  FP32: the filter minus the
+    // identity is applied to the shifted row and its result added to the
+    // FP64 row.
     const int nfp = (a.nvar + 1) / 2;
     for (int q = 0; q < nfp; q++) {
         const int v = 2 * q, w = v + 1 < a.nvar ? v + 1 : -1;
-        yr_load<L>(A, fc(a.uu, v), w >= 0 ? fc(a.uu, w) : nullptr, j, valid);
-        yr_op<L>(a, A, j, valid, a.sf, f(a.uu, v), w >= 0 ? f(a.uu, w) : nullptr);
+        double *ra = su(v), *rb = w >= 0 ? su(w) : nullptr;
+        const double ca = sh(ra), cb = rb ? sh(rb) : 0.0;
+        yr_load<L, T>(A, ra, rb, ca, cb, j, valid);
+        if constexpr (MIX)
+            yr_op<L, T, true>(tw, A, j, valid, reinterpret_cast<const C *>(a.sfd32), ra, rb);
+        else
+            yr_op<L, T, false>(tw, A, j, valid, reinterpret_cast<const C *>(a.sf), ra, rb);
     }
 }
 
-template <int L>
+template <int L, typename T>
 static int launch_yrow_l(Ctx *c, const YRArgs &a, double bytes)
 {
-    using G = YRGeom<L>;
+    using G = YRGeom<L, T>;
     const size_t smem = G::SMEM;
     static bool attr_done[64] = {false};  // per device
     int dev = 0;
     MHD_CUDA_TRY(cudaGetDevice(&dev));
     if (dev < 0 || dev >= 64) return mhd_set_error(MHDGPU_ERR_UNSUPPORTED);
     if (!attr_done[dev]) {
-        MHD_CUDA_TRY(cudaFuncSetAttribute(yrow_kernel<L>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                          (int)smem));
+        MHD_CUDA_TRY(cudaFuncSetAttribute(yrow_kernel<L, T>,
+                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         attr_done[dev] = true;
     }
     const unsigned grid = (unsigned)((c->nx + G::ROWS - 1) / G::ROWS);
     prof_begin(c, KC_FUSED_Y, bytes);
-    yrow_kernel<L><<<grid, G::T * G::ROWS, smem, c->stream>>>(a);
+    yrow_kernel<L, T><<<grid, G::T_ * G::ROWS, smem, c->stream>>>(a);
     prof_end(c);
     MHD_CHECK_LAUNCH();
     return MHDGPU_OK;
@@ -242,6 +299,10 @@ int launch_yrow(Ctx *c, int iRK, int last_stage)
     a.s1 = reinterpret_cast<const double2 *>(c->ysym_d1);
     a.s2 = reinterpret_cast<const double2 *>(c->ysym_d2);
     a.sf = reinterpret_cast<const double2 *>(c->ysym_f);
+    a.tw32 = c->ytab32;
+    a.s1_32 = c->ytab32 + c->ny;
+    a.s2_32 = c->ytab32 + 2 * c->ny;
+    a.sfd32 = c->ytab32 + 3 * c->ny;
     a.nx = c->nx;
     a.ny = c->ny;
     a.nvar = c->nvar;
@@ -260,16 +321,32 @@ int launch_yrow(Ctx *c, int iRK, int last_stage)
     const double bytes = (double)c->nx * c->ny * 8.0 *
                          (c->nvar + nx_der + (a.read_rk ? c->nvar : 0) + c->nvar +
                           (a.write_rk ? c->nvar : 0));
+    if (c->mixed) {
+        // the x derivatives are read as floats: half their bytes
+        const double b = bytes - (double)c->nx * c->ny * 4.0 * nx_der;
+        switch (c->ny) {
+        case 16: return launch_yrow_l<4, float>(c, a, b);
+        case 32: return launch_yrow_l<5, float>(c, a, b);
+        case 64: return launch_yrow_l<6, float>(c, a, b);
+        case 128: return launch_yrow_l<7, float>(c, a, b);
+        case 256: return launch_yrow_l<8, float>(c, a, b);
+        case 512: return launch_yrow_l<9, float>(c, a, b);
+        case 1024: return launch_yrow_l<10, float>(c, a, b);
+        case 2048: return launch_yrow_l<11, float>(c, a, b);
+        case 4096: return launch_yrow_l<12, float>(c, a, b);
+        default: return mhd_set_error(MHDGPU_ERR_UNSUPPORTED);
+        }
+    }
     switch (c->ny) {
-    case 16: return launch_yrow_l<4>(c, a, bytes);
-    case 32: return launch_yrow_l<5>(c, a, bytes);
-    case 64: return launch_yrow_l<6>(c, a, bytes);
-    case 128: return launch_yrow_l<7>(c, a, bytes);
-    case 256: return launch_yrow_l<8>(c, a, bytes);
-    case 512: return launch_yrow_l<9>(c, a, bytes);
-    case 1024: return launch_yrow_l<10>(c, a, bytes);
-    case 2048: return launch_yrow_l<11>(c, a, bytes);
-    case 4096: return launch_yrow_l<12>(c, a, bytes);
+    case 16: return launch_yrow_l<4, double>(c, a, bytes);
+    case 32: return launch_yrow_l<5, double>(c, a, bytes);
+    case 64: return launch_yrow_l<6, double>(c, a, bytes);
+    case 128: return launch_yrow_l<7, double>(c, a, bytes);
+    case 256: return launch_yrow_l<8, double>(c, a, bytes);
+    case 512: return launch_yrow_l<9, double>(c, a, bytes);
+    case 1024: return launch_yrow_l<10, double>(c, a, bytes);
+    case 2048: return launch_yrow_l<11, double>(c, a, bytes);
+    case 4096: return launch_yrow_l<12, double>(c, a, bytes);
     default: return mhd_set_error(MHDGPU_ERR_UNSUPPORTED);
     }
 }

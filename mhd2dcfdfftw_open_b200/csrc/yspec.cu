@@ -186,6 +186,17 @@ int yspec_setup(Ctx *c)
     c->ysym_d1 = reinterpret_cast<double *>(sym);
     c->ysym_d2 = reinterpret_cast<double *>(sym + N);
     c->ysym_f = reinterpret_cast<double *>(sym + 2 * N);
+    // FP32 tables: twiddles, the two derivative symbols, and the filter
+    // symbol minus the identity (1/N with the unnormalised transforms)
+    std::vector<float2> t32(4 * N);
+    for (long k = 0; k < N; k++) {
+        t32[k] = make_float2((float)tw[k].x, (float)tw[k].y);
+        t32[N + k] = make_float2((float)s1[k].x, (float)s1[k].y);
+        t32[2 * N + k] = make_float2((float)s2[k].x, (float)s2[k].y);
+        t32[3 * N + k] = make_float2((float)(sf[k].x - 1.0 / (double)N), (float)sf[k].y);
+    }
+    MHD_CUDA_TRY(cudaMalloc(&c->ytab32, sizeof(float2) * 4 * N));
+    MHD_CUDA_TRY(cudaMemcpy(c->ytab32, t32.data(), sizeof(float2) * 4 * N, cudaMemcpyHostToDevice));
     MHD_CUDA_TRY(cudaFuncSetAttribute(yspec_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       (int)(sizeof(double2) * 8192)));
     return MHDGPU_OK;
@@ -195,6 +206,8 @@ void yspec_free(Ctx *c)
 {
     cudaFree(c->tw);
     cudaFree(c->ysym_d1);
+    cudaFree(c->ytab32);
+    c->ytab32 = nullptr;
     c->tw = nullptr;
     c->ysym_d1 = c->ysym_d2 = c->ysym_f = nullptr;
 }

@@ -43,8 +43,12 @@ EXPORTED = (
     "mhdgpu_rk_execute", "mhdgpu_filtering", "mhdgpu_calc_dt", "mhdgpu_check_divb",
     "mhdgpu_get_cleaning_speeds", "mhdgpu_stage", "mhdgpu_steps", "mhdgpu_steps_fused",
     "mhdgpu_diagnostics", "mhdgpu_stream", "mhdgpu_launch_count", "mhdgpu_profile",
-    "mhdgpu_profile_read",
+    "mhdgpu_profile_read", "mhdgpu_set_precision",
 )
+
+# arithmetic of the fused steps (mhdgpu_set_precision)
+PRECISION_FP64 = 0
+PRECISION_MIXED = 1
 
 # kernel classes of mhdgpu_profile_read
 KCLASSES = ("xsolve", "yspec", "pointwise", "reduce", "fused_x", "fused_y")
@@ -90,6 +94,7 @@ def load_library(path: str = LIB_PATH):
     L.mhdgpu_stage.argtypes = [vp, ctypes.c_int]
     L.mhdgpu_steps.argtypes = [vp, ctypes.c_int, ctypes.c_double, dp]
     L.mhdgpu_steps_fused.argtypes = [vp, ctypes.c_int, ctypes.c_double, dp]
+    L.mhdgpu_set_precision.argtypes = [vp, ctypes.c_int]
     L.mhdgpu_diagnostics.argtypes = [vp, dp, dp, ctypes.POINTER(ctypes.c_int)]
     L.mhdgpu_stream.argtypes = [vp]
     L.mhdgpu_stream.restype = vp
@@ -224,6 +229,13 @@ class Domain:
         f = self.lib.mhdgpu_steps_fused if fused else self.lib.mhdgpu_steps
         self._check(f(self.h, int(nsteps), float(dt_fixed), ctypes.byref(d)))
         return d.value
+
+    def set_precision(self, mixed):
+        """Arithmetic of the fused steps: FP64 (False, the default) or mixed
+        precision (True: FP32 sweeps, butterflies and fluxes, FP64 state and
+        RK3 accumulation)."""
+        self._check(self.lib.mhdgpu_set_precision(
+            self.h, PRECISION_MIXED if mixed else PRECISION_FP64))
 
     def diagnostics(self):
         e, h, fin = ctypes.c_double(), ctypes.c_double(), ctypes.c_int()

@@ -1,0 +1,89 @@
+"""Host logic of the serving layer (no GPU): admission by HBM footprint,
+first-come-first-served order, concurrency bounded by the slots, request
+streams and the latency summary."""
+import threading
+import time
+
+import numpy as np
+
+from mhd2dcfdfftw_open_b200 import serving as S
+
+
+class FakeServer(S.Server):
+    """Jobs sleep instead of running on a GPU; records what ran together."""
+
+    def __init__(self, *a, **k):
+        self.lock = threading.Lock()
+        self.active = []
+        self.peak_bytes = 0.0
+        self.peak_jobs = 0
+        self.order = []
+        super().__init__(*a, **k)
+
+    def _run(self, req, admitted):
+        fp = S.footprint_bytes(req.nx, req.ny)
+        with self.lock:
+            self.active.append(fp)
+            self.order.append(req.rid)
+            self.peak_bytes = max(self.peak_bytes, sum(self.active))
+            self.peak_jobs = max(self.peak_jobs, len(self.active))
+        time.sleep(0.002 * req.steps / 100)
+        with self.lock:
+            self.active.remove(fp)
+        return S.Result(req.rid, req.nx * req.ny, req.steps, req.arrival, admitted,
+                        self.clock(), 1e-3, 1.0)
+
+
+def test_footprint_counts_the_reference_arrays():
+    assert S.footprint_bytes(256, 256) == 64 * 256 * 256 * 8 + (8 << 20)
+    assert S.footprint_bytes(256, 256, nvar=9) == 69 * 256 * 256 * 8 + (8 << 20)
+
+
+def test_admission_respects_budget_and_slots():
+    reqs = S.draw_requests(40, seed=7, rate=0.0, sizes=S.ENSEMBLE_SIZES,
+                           inverse_cells=False, steps=(100, 300))
+    budget = 3 * S.footprint_bytes(1024, 1024)
+    srv = FakeServer(budget, slots=5)
+    srv.start_clock()
+    for r in reqs:
+        srv.submit(r)
+    srv.drain()
+    assert len(srv.results) == 40
+    assert srv.peak_bytes <= budget
+    assert 1 < srv.peak_jobs <= 5
+    assert srv.order == sorted(srv.order)  # first come, first served
+
+
+def test_oversized_request_is_rejected():
+    srv = FakeServer(S.footprint_bytes(256, 256), slots=1)
+    try:
+        r = S.Request(0, 512, 512, 10)
+        try:
+            srv.submit(r)
+            raise AssertionError("accepted a job above the budget")
+        except ValueError:
+            pass
+    finally:
+        srv.drain()
+
+
+def test_request_stream_is_seeded_and_poisson():
+    a = S.draw_requests(500, seed=5, rate=20.0)
+    b = S.draw_requests(500, seed=5, rate=20.0)
+    assert [(r.nx, r.steps, r.kind, r.arrival) for r in a] == \
+           [(r.nx, r.steps, r.kind, r.arrival) for r in b]
+    gaps = np.diff([0.0] + [r.arrival for r in a])
+    assert abs(gaps.mean() - 1 / 20.0) < 0.01
+    cells = np.array([r.nx * r.ny for r in a])
+    # probability proportional to 1/cells: the smallest size dominates
+    assert (cells == 128 * 128).mean() > 0.5
+    assert all(100 <= r.steps <= 2000 for r in a)
+    assert all(0.0 <= r.di <= 0.1 and 1e-4 <= r.eta <= 1e-3 and r.eta == r.nu for r in a)
+
+
+def test_summary_percentiles():
+    res = [S.Result(i, 100, 10, 0.0, 0.0, float(i + 1), 1e-3, 1.0) for i in range(100)]
+    s = S.summarize(res, 100.0)
+    assert s["p50_latency_s"] == np.percentile(np.arange(1, 101), 50)
+    assert s["p99_latency_s"] == np.percentile(np.arange(1, 101), 99)
+    assert s["cell_updates_per_s"] == 100 * 100 * 10 / 100.0
