@@ -128,6 +128,16 @@ int mhdgpu_steps_fused(mhdgpu_ctx *ctx, int nsteps, double dt_fixed, double *dt_
 enum { MHDGPU_PRECISION_FP64 = 0, MHDGPU_PRECISION_MIXED = 1 };
 int mhdgpu_set_precision(mhdgpu_ctx *ctx, int precision);
 
+/* Autotuner of the fused x pass (no counterpart in the reference): times the
+ * pass for each tile width this grid admits (8, 16, 32 columns per CTA; the
+ * rows per CTA and the cluster size follow from it) at the context's current
+ * precision, keeps the fastest and remembers it for contexts of the same
+ * shape and precision created later in this process.  The state is only
+ * read; the derivative arrays are overwritten.  *columns_out: the width
+ * chosen (may be NULL).  MHDGPU_ERR_UNSUPPORTED when the grid has no fused x
+ * pass. */
+int mhdgpu_autotune(mhdgpu_ctx *ctx, int *columns_out);
+
 /* --- diagnostics -------------------------------------------------------- */
 /* total energy, cross helicity (sums times dx*dy) and max|divB| of the last
  * computed derivatives; *finite = 0 if the state holds NaN/Inf or rho,p<=0 */

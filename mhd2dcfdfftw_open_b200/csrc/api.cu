@@ -7,6 +7,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <mutex>
 #include <new>
 
 #include "common.cuh"
@@ -95,12 +96,31 @@ static int fields_of(const Ctx *c, int which)
     }
 }
 
+// Stream capture and the calls that synchronize the device (cudaFree) or
+// allocate must not interleave across threads: a device-wide synchronization
+// during another thread's capture invalidates that capture.  Contexts served
+// from several threads therefore take this lock around capture, creation and
+// destruction (all short, host-side).
+static std::mutex g_device_mu;
+
+static void destroy_locked(mhdgpu_ctx *h);
+
 extern "C" void mhdgpu_destroy(mhdgpu_ctx *h)
+{
+    std::lock_guard<std::mutex> lock(g_device_mu);
+    destroy_locked(h);
+}
+
+// mhdgpu_destroy with g_device_mu held
+static void destroy_locked(mhdgpu_ctx *h)
 {
     Ctx *c = reinterpret_cast<Ctx *>(h);
     if (!c) return;
     cudaSetDevice(c->device);
     if (c->stream) cudaStreamSynchronize(c->stream);
+    for (int i = 0; i < 2; i++)
+        for (int j = 0; j < 2; j++)
+            if (c->step_graph[i][j]) cudaGraphExecDestroy(c->step_graph[i][j]);
     mhd::fused_free(c);
     mhd::xsolve_free(c);
     mhd::yspec_free(c);
@@ -128,6 +148,7 @@ static bool valid_params(const mhdgpu_params *p)
 
 extern "C" int mhdgpu_create(const mhdgpu_params *p, int device, mhdgpu_ctx **out)
 {
+    std::lock_guard<std::mutex> lock(g_device_mu);
     if (!out) return mhd_set_error(MHDGPU_ERR_INVALID);
     *out = nullptr;
     if (!valid_params(p)) return mhd_set_error(MHDGPU_ERR_INVALID);
@@ -150,7 +171,7 @@ extern "C" int mhdgpu_create(const mhdgpu_params *p, int device, mhdgpu_ctx **ou
     c->Ch = c->Cp = 0.0;
     int rc = MHDGPU_OK;
     auto fail = [&](int s) {
-        mhdgpu_destroy(reinterpret_cast<mhdgpu_ctx *>(c));
+        destroy_locked(reinterpret_cast<mhdgpu_ctx *>(c));
         return mhd_set_error(s);
     };
     if (cudaSetDevice(device) != cudaSuccess) return fail(MHDGPU_ERR_CUDA);
@@ -178,7 +199,11 @@ extern "C" int mhdgpu_create(const mhdgpu_params *p, int device, mhdgpu_ctx **ou
     if ((rc = mhd::xsolve_setup(c)) != MHDGPU_OK) return fail(rc);
     if ((rc = mhd::yspec_setup(c)) != MHDGPU_OK) return fail(rc);
     if ((rc = mhd::fused_setup(c)) != MHDGPU_OK) return fail(rc);
-    if (cudaDeviceSynchronize() != cudaSuccess) return fail(MHDGPU_ERR_CUDA);
+    // set-up work is on this context's stream and the legacy stream; other
+    // contexts' streams keep running
+    if (cudaStreamSynchronize(c->stream) != cudaSuccess ||
+        cudaStreamSynchronize(cudaStreamLegacy) != cudaSuccess)
+        return fail(MHDGPU_ERR_CUDA);
     *out = reinterpret_cast<mhdgpu_ctx *>(c);
     return MHDGPU_OK;
 }
@@ -439,6 +464,33 @@ extern "C" int mhdgpu_steps(mhdgpu_ctx *h, int nsteps, double dt_fixed, double *
 // (divBcleaning == 1) needs d/dx, d/dy of divB inside the stage, and grids the
 // fused x pass cannot tile (an odd nx with 8 columns), run through the
 // operator stage instead.
+// One fused RK3 step under device step control: the three fused stages and,
+// with CFL control or hyperbolic cleaning, the x filter they leave pending
+// and calcDt for the next step, all on the device.
+static int fused_step_dev(Ctx *c, bool need_dt, bool keep_dt)
+{
+    for (int k = 0; k < 3; k++) TRY(mhd::fused_stage(c, k, 0, k == 2));
+    if (need_dt) {
+        TRY(settle(c));
+        TRY(mhd::launch_calc_dt_dev(c, keep_dt));
+    }
+    return MHDGPU_OK;
+}
+
+// Steps through the fused stage (fused.cu).  Diffusive cleaning
+// (divBcleaning == 1) needs d/dx, d/dy of divB inside the stage, and grids the
+// fused x pass cannot tile (an odd nx with 8 columns), run through the
+// operator stage instead.
+//
+// With the row kernel (16 <= ny <= 4096) the step control stays on the
+// device: dt (and Ch, Cp) live in dscal, the y pass forms cc = c_k dt and
+// dd = d_k dt there, calcDt runs on the device (the reference's arithmetic
+// and hysteresis, timeAdvance.c:38-153), and dudtRK needs no clearing between
+// steps (the first stage neither reads it nor needs it zero).  A step whose
+// entry state is the steady one (CFL: filter settled; fixed dt: filter
+// pending) is captured once per context, precision and dt mode as a CUDA graph
+// and replayed; the host waits only at the end.  Profiling runs the same
+// launches without the graph.
 extern "C" int mhdgpu_steps_fused(mhdgpu_ctx *h, int nsteps, double dt_fixed, double *dt_io)
 {
     CTX_OR_FAIL(h);
@@ -449,17 +501,98 @@ extern "C" int mhdgpu_steps_fused(mhdgpu_ctx *h, int nsteps, double dt_fixed, do
     if (nsteps > 0) c->deriv_fp32 = c->mixed;
     const bool need_dt = dt_fixed <= 0 || c->p.divBcleaning == 2;
     double dt = dt_io ? *dt_io : 0.0;
-    if (need_dt) TRY(settle(c));
-    TRY(next_dt(h, c, dt_fixed, &dt));
-    TRY(mhdgpu_rk_init(h, dt));
-    for (int s = 0; s < nsteps; s++) {
-        for (int k = 0; k < 3; k++) TRY(mhd::fused_stage(c, k, s == 0 && k == 0, k == 2));
+    if (!mhd::yrow_supported(c)) {  // host step control (operator y sequence)
         if (need_dt) TRY(settle(c));
         TRY(next_dt(h, c, dt_fixed, &dt));
         TRY(mhdgpu_rk_init(h, dt));
+        for (int s = 0; s < nsteps; s++) {
+            for (int k = 0; k < 3; k++) TRY(mhd::fused_stage(c, k, s == 0 && k == 0, k == 2));
+            if (need_dt) TRY(settle(c));
+            TRY(next_dt(h, c, dt_fixed, &dt));
+            TRY(mhdgpu_rk_init(h, dt));
+        }
+        TRY(settle(c));
+        if (dt_io) *dt_io = dt;
+        MHD_CUDA_TRY(cudaStreamSynchronize(c->stream));
+        return check_flag(c);
     }
+
+    // device step control
+    const bool fixed = dt_fixed > 0;
+    const double dt0 = fixed ? dt_fixed : dt;
+    MHD_CUDA_TRY(cudaMemcpyAsync(c->dscal, &dt0, sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    if (need_dt) {
+        TRY(settle(c));
+        TRY(mhd::launch_calc_dt_dev(c, fixed));
+    }
+    c->dev_dt = 1;
+    const int gm = c->mixed ? 1 : 0, gd = fixed ? 1 : 0;
+    int rc = MHDGPU_OK;
+    for (int s = 0; s < nsteps && rc == MHDGPU_OK; s++) {
+        // the steady entry state: filter settled with CFL control, pending otherwise
+        const bool steady = need_dt ? !c->fused_pending_filter : c->fused_pending_filter != 0;
+        if (!steady || c->prof_on || s == 0) {
+            rc = fused_step_dev(c, need_dt, fixed);
+            continue;
+        }
+        if (!c->step_graph[gm][gd]) {
+            std::lock_guard<std::mutex> lock(g_device_mu);
+            const long l0 = c->launches;
+            cudaGraph_t g = nullptr;
+            if (cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+                rc = mhd_set_error(MHDGPU_ERR_CUDA);
+                break;
+            }
+            const int rs = fused_step_dev(c, need_dt, fixed);
+            const cudaError_t ec = cudaStreamEndCapture(c->stream, &g);
+            if (rs || ec != cudaSuccess ||
+                cudaGraphInstantiate(&c->step_graph[gm][gd], g, 0) != cudaSuccess) {
+                if (g) cudaGraphDestroy(g);
+                c->step_graph[gm][gd] = nullptr;
+                rc = rs ? rs : mhd_set_error(MHDGPU_ERR_CUDA);
+                break;
+            }
+            cudaGraphDestroy(g);
+            c->step_graph_launches[gm][gd] = c->launches - l0;
+            c->launches = l0;  // captured, not yet run
+        }
+        if (cudaGraphLaunch(c->step_graph[gm][gd], c->stream) != cudaSuccess) {
+            rc = mhd_set_error(MHDGPU_ERR_CUDA);
+            break;
+        }
+        c->launches += c->step_graph_launches[gm][gd];
+    }
+    c->dev_dt = 0;
+    TRY(rc);
     TRY(settle(c));
+    double hs[3];
+    MHD_CUDA_TRY(cudaMemcpyAsync(hs, c->dscal, sizeof hs, cudaMemcpyDeviceToHost, c->stream));
+    MHD_CUDA_TRY(cudaStreamSynchronize(c->stream));
+    if (!fixed) dt = hs[0];
+    else dt = dt_fixed;
+    if (c->p.divBcleaning == 2) {
+        c->Ch = hs[1];
+        c->Cp = hs[2];
+    }
+    TRY(mhdgpu_rk_init(h, dt));  // the host coefficients and dudtRK = 0, as rkInit leaves them
     if (dt_io) *dt_io = dt;
+    MHD_CUDA_TRY(cudaStreamSynchronize(c->stream));
+    return check_flag(c);
+}
+
+extern "C" int mhdgpu_autotune(mhdgpu_ctx *h, int *columns_out)
+{
+    CTX_OR_FAIL(h);
+    if (settle(c)) return mhdgpu_last_error();
+    TRY(mhd::xline_autotune(c, columns_out));
+    // the captured steps hold the previous tiling
+    std::lock_guard<std::mutex> lock(g_device_mu);
+    for (int i = 0; i < 2; i++)
+        for (int j = 0; j < 2; j++)
+            if (c->step_graph[i][j]) {
+                cudaGraphExecDestroy(c->step_graph[i][j]);
+                c->step_graph[i][j] = nullptr;
+            }
     MHD_CUDA_TRY(cudaStreamSynchronize(c->stream));
     return check_flag(c);
 }

@@ -71,6 +71,12 @@ struct Ctx {
     float2 *ytab32;
     int mixed;       // fused steps in mixed precision (FP32 operators, FP64 state)
     int deriv_fp32;  // the derivative arrays hold FP32 scratch of mixed steps
+    // device step control of the fused steps: dt, Ch, Cp live in dscal and
+    // the y pass forms its RK3 coefficients there; one step is captured as a
+    // CUDA graph per (precision, CFL or fixed dt) and replayed
+    int dev_dt;
+    cudaGraphExec_t step_graph[2][2];
+    long step_graph_launches[2][2];
     // scalars on the device: [0] dt, [1] Ch, [2] Cp, [3..] scratch
     double *dscal;
     double *dred;                // block partials of reductions
@@ -134,6 +140,7 @@ int launch_divb(Ctx *c, double *out);
 int launch_rhs(Ctx *c);
 int launch_rk(Ctx *c, int iRK);
 int launch_calc_dt(Ctx *c, double dt0, double *dt_out);
+int launch_calc_dt_dev(Ctx *c, int keep_dt);
 int launch_max_divb(Ctx *c, double *out);
 int launch_diagnostics(Ctx *c, double *energy, double *ch, int *finite);
 int xline_setup(Ctx *c);
@@ -142,4 +149,5 @@ int fused_setup(Ctx *c);
 void fused_free(Ctx *c);
 int fused_stage(Ctx *c, int iRK, int first_stage_of_run, int last_stage);
 bool yrow_supported(const Ctx *c);
+int xline_autotune(Ctx *c, int *w_out);
 }  // namespace mhd

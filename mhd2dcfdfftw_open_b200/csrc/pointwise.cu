@@ -137,8 +137,11 @@ __global__ void dt_partial_kernel(DtArgs a)
 // hyperbolic cleaning scal[1] = Ch = max(cmaxx, cmaxy) of the LAST cell of
 // the reference's loop (timeAdvance.c:107-112) and scal[2] = Cp = sqrt(Cr Ch)
 // (divBcleaning.c:4-10).
+// scal[0] = the new dt (hysteresis of timeAdvance.c:144-151 around dt0;
+// dt0 is scal[0] itself with dev_dt, and scal[0] is left alone with keep_dt),
+// scal[1..2] = Ch, Cp of hyperbolic cleaning
 __global__ void dt_final_kernel(DtArgs a, int nparts, double cfl, double dt0, int cleaning,
-                                double *scal)
+                                double *scal, int dev_dt, int keep_dt)
 {
     double mn = INFINITY;
     for (int i = threadIdx.x; i < nparts; i += blockDim.x) mn = fmin(mn, a.part[i]);
@@ -150,7 +153,8 @@ __global__ void dt_final_kernel(DtArgs a, int nparts, double cfl, double dt0, in
         double v = INFINITY;
         for (int w = 0; w < (int)(blockDim.x / 32); w++) v = fmin(v, sm[w]);
         double dtmin = v * cfl;
-        scal[0] = (dt0 < 0.98 * dtmin || dt0 > 1.02 * dtmin) ? dtmin : dt0;
+        if (dev_dt) dt0 = scal[0];
+        if (!keep_dt) scal[0] = (dt0 < 0.98 * dtmin || dt0 > 1.02 * dtmin) ? dtmin : dt0;
         if (cleaning == 2) {
             double cx, cy;
             cell_speeds(a, a.plane - 1, cx, cy);
@@ -304,7 +308,7 @@ int launch_rk(Ctx *c, int iRK)
     return MHDGPU_OK;
 }
 
-int launch_calc_dt(Ctx *c, double dt0, double *dt_out)
+static DtArgs dt_args(Ctx *c)
 {
     DtArgs a;
     a.uu = c->arr[MHDGPU_UU];
@@ -318,6 +322,15 @@ int launch_calc_dt(Ctx *c, double dt0, double *dt_out)
     a.visc = c->p.viscosity;
     a.hall = c->p.Hall;
     a.part = c->dred;
+    return a;
+}
+
+// calcDt on the device only: dt stays in dscal[0] (the previous dt there is
+// dt0 of the hysteresis; keep_dt leaves a fixed dt untouched), Ch and Cp in
+// dscal[1..2]; nothing is read back, so it can run inside a captured step.
+int launch_calc_dt_dev(Ctx *c, int keep_dt)
+{
+    DtArgs a = dt_args(c);
     int g = grid_for(c, a.plane);
     if (g > c->nred) g = c->nred;
     prof_begin(c, KC_REDUCE, 7.0 * a.plane * 8.0);
@@ -325,7 +338,24 @@ int launch_calc_dt(Ctx *c, double dt0, double *dt_out)
     prof_end(c);
     MHD_CHECK_LAUNCH();
     prof_begin(c, KC_REDUCE, 0.0);
-    dt_final_kernel<<<1, 1024, 0, c->stream>>>(a, g, c->p.cfl, dt0, c->p.divBcleaning, c->dscal);
+    dt_final_kernel<<<1, 1024, 0, c->stream>>>(a, g, c->p.cfl, 0.0, c->p.divBcleaning, c->dscal, 1,
+                                               keep_dt);
+    prof_end(c);
+    MHD_CHECK_LAUNCH();
+    return MHDGPU_OK;
+}
+
+int launch_calc_dt(Ctx *c, double dt0, double *dt_out)
+{
+    DtArgs a = dt_args(c);
+    int g = grid_for(c, a.plane);
+    if (g > c->nred) g = c->nred;
+    prof_begin(c, KC_REDUCE, 7.0 * a.plane * 8.0);
+    dt_partial_kernel<<<g, PT, 0, c->stream>>>(a);
+    prof_end(c);
+    MHD_CHECK_LAUNCH();
+    prof_begin(c, KC_REDUCE, 0.0);
+    dt_final_kernel<<<1, 1024, 0, c->stream>>>(a, g, c->p.cfl, dt0, c->p.divBcleaning, c->dscal, 0, 0);
     prof_end(c);
     MHD_CHECK_LAUNCH();
     double h[3];

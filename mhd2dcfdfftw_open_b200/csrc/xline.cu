@@ -11,7 +11,8 @@
 //   * field v+1 is staged into the second of two shared-memory tiles by the
 //     TMA engine (cp.async.bulk, one W*8-byte copy per row, mbarrier
 //     completion) while field v is solved;
-//   * 1024 threads per CTA: thread (column, sub-chunk) keeps its 8 rows of a
+//   * 512 threads per CTA, two CTAs per SM (one CTA's barrier waits overlap
+//     the other's sweeps): thread (column, sub-chunk) keeps its 8 rows of a
 //     recurrence in registers; the exact inflows of each sub-chunk come from
 //     a warp-shuffle scan of the sub-chunk (end value, product) pairs inside
 //     the CTA and of the CTA pairs across the cluster, read through
@@ -29,6 +30,9 @@
 #include <cmath>
 #include <cstdlib>
 #include <cstring>
+#include <map>
+#include <mutex>
+#include <tuple>
 #include <vector>
 
 #include "common.cuh"
@@ -39,13 +43,13 @@ namespace cg = cooperative_groups;
 namespace mhd {
 
 #ifndef MHD_XLINE_THREADS
-#define MHD_XLINE_THREADS 1024
+#define MHD_XLINE_THREADS 512
 #endif
 #ifndef MHD_XLINE_ROWS
 #define MHD_XLINE_ROWS 8
 #endif
 #ifndef MHD_XLINE_MINB
-#define MHD_XLINE_MINB 1
+#define MHD_XLINE_MINB 2  // CTAs per SM the registers are budgeted for
 #endif
 constexpr int XL_T = MHD_XLINE_THREADS;  // threads per CTA
 constexpr int XL_S = MHD_XLINE_ROWS;     // rows of a recurrence per thread
@@ -121,60 +125,62 @@ __device__ __forceinline__ void xl_scan(const XLSmem<T> &s, T *cta, int off, boo
     // carry the identity pair (0, 1)
     constexpr int K = NSUB >= 32 ? NSUB / 32 : 1;
     static_assert(NSUB < 32 || NSUB % 32 == 0, "sub-chunks per column must fill whole warps");
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    if (warp >= W) return;
-    const int base = warp * (NSUB + 1);
-    T E[NR], P = (T)1;
+    const int lane = threadIdx.x & 31;
+    // warp w scans columns w, w + (warps per CTA), ...
+    for (int warp = threadIdx.x >> 5; warp < W; warp += XL_T / 32) {
+        const int base = warp * (NSUB + 1);
+        T E[NR], P = (T)1;
 #pragma unroll
-    for (int r = 0; r < NR; r++) E[r] = (T)0;
+        for (int r = 0; r < NR; r++) E[r] = (T)0;
 #pragma unroll
-    for (int jq = 0; jq < K; jq++) {
-        int q = lane * K + jq;
-        if (q >= NSUB) break;
-        int sidx = reverse ? NSUB - 1 - q : q;
-        const T p = s.aggP[base + sidx];
+        for (int jq = 0; jq < K; jq++) {
+            int q = lane * K + jq;
+            if (q >= NSUB) break;
+            int sidx = reverse ? NSUB - 1 - q : q;
+            const T p = s.aggP[base + sidx];
 #pragma unroll
-        for (int r = 0; r < NR; r++) E[r] = s.aggE[r][base + sidx] + p * E[r];
-        P = p * P;
-    }
-    // every lane takes part in every shuffle (full mask)
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-        T Eo[NR];
-#pragma unroll
-        for (int r = 0; r < NR; r++) Eo[r] = __shfl_up_sync(0xffffffffu, E[r], o);
-        const T Po = __shfl_up_sync(0xffffffffu, P, o);
-        if (lane >= o) {
-#pragma unroll
-            for (int r = 0; r < NR; r++) E[r] = E[r] + P * Eo[r];
-            P = P * Po;
+            for (int r = 0; r < NR; r++) E[r] = s.aggE[r][base + sidx] + p * E[r];
+            P = p * P;
         }
-    }
-    T Ex[NR];
+        // every lane takes part in every shuffle (full mask)
 #pragma unroll
-    for (int r = 0; r < NR; r++) {
-        const T e = __shfl_up_sync(0xffffffffu, E[r], 1);
-        Ex[r] = lane == 0 ? (T)0 : e;
-    }
-    const T pxs = __shfl_up_sync(0xffffffffu, P, 1);
-    T Px = lane == 0 ? (T)1 : pxs;
-    if (lane == 31) {
+        for (int o = 1; o < 32; o <<= 1) {
+            T Eo[NR];
 #pragma unroll
-        for (int r = 0; r < NR; r++) cta[(off + r) * W + warp] = E[r];
-        cta[(off + 2) * W + warp] = P;
-    }
+            for (int r = 0; r < NR; r++) Eo[r] = __shfl_up_sync(0xffffffffu, E[r], o);
+            const T Po = __shfl_up_sync(0xffffffffu, P, o);
+            if (lane >= o) {
 #pragma unroll
-    for (int jq = 0; jq < K; jq++) {
-        int q = lane * K + jq;
-        if (q >= NSUB) break;
-        int sidx = reverse ? NSUB - 1 - q : q;
+                for (int r = 0; r < NR; r++) E[r] = E[r] + P * Eo[r];
+                P = P * Po;
+            }
+        }
+        T Ex[NR];
 #pragma unroll
-        for (int r = 0; r < NR; r++) s.preE[r][base + sidx] = Ex[r];
-        s.preP[base + sidx] = Px;
-        const T p = s.aggP[base + sidx];
+        for (int r = 0; r < NR; r++) {
+            const T e = __shfl_up_sync(0xffffffffu, E[r], 1);
+            Ex[r] = lane == 0 ? (T)0 : e;
+        }
+        const T pxs = __shfl_up_sync(0xffffffffu, P, 1);
+        T Px = lane == 0 ? (T)1 : pxs;
+        if (lane == 31) {
 #pragma unroll
-        for (int r = 0; r < NR; r++) Ex[r] = s.aggE[r][base + sidx] + p * Ex[r];
-        Px = p * Px;
+            for (int r = 0; r < NR; r++) cta[(off + r) * W + warp] = E[r];
+            cta[(off + 2) * W + warp] = P;
+        }
+#pragma unroll
+        for (int jq = 0; jq < K; jq++) {
+            int q = lane * K + jq;
+            if (q >= NSUB) break;
+            int sidx = reverse ? NSUB - 1 - q : q;
+#pragma unroll
+            for (int r = 0; r < NR; r++) s.preE[r][base + sidx] = Ex[r];
+            s.preP[base + sidx] = Px;
+            const T p = s.aggP[base + sidx];
+#pragma unroll
+            for (int r = 0; r < NR; r++) Ex[r] = s.aggE[r][base + sidx] + p * Ex[r];
+            Px = p * Px;
+        }
     }
 }
 
@@ -736,24 +742,55 @@ static int xl_attrs(int C)
     return MHDGPU_OK;
 }
 
+// Tile widths picked by xline_autotune, per grid shape and precision, for
+// the contexts this process creates later.
+struct XLTuneKey {
+    long nx, ny;
+    int nvar, mixed;
+    bool operator<(const XLTuneKey &o) const
+    {
+        return std::tie(nx, ny, nvar, mixed) < std::tie(o.nx, o.ny, o.nvar, o.mixed);
+    }
+};
+static std::map<XLTuneKey, int> g_xl_tuned;
+static std::mutex g_xl_tuned_mu;
+
+static int xl_configure(Ctx *c, int W);
+
 int xline_setup(Ctx *c)
 {
     int rc = xline_tables(c);
     if (rc) return rc;
     const long n = c->nx;
     // One CTA holds up to RCAP rows of W columns.  Short lines take W = 32 in
-    // one CTA; longer lines take W = 8 (1024 rows per CTA), which keeps the
-    // clusters small (4 CTAs for 4096 rows) so more of them fit on the GPU.
+    // one CTA; longer lines take W = 8 (512 rows per CTA: clusters of 8 CTAs
+    // for 4096 rows, 16 for 8192), which keeps the clusters' SM footprint
+    // small so more of them fit on the GPU.
     // MHDGPU_XLINE_W (8, 16 or 32) overrides the choice.
+    // A width picked by xline_autotune for this shape comes first.
     int W = n <= XLGeom<32>::RCAP ? 32 : 8;
+    {
+        std::lock_guard<std::mutex> lock(g_xl_tuned_mu);
+        auto it = g_xl_tuned.find(XLTuneKey{c->nx, c->ny, c->nvar, c->mixed});
+        if (it != g_xl_tuned.end()) W = it->second;
+    }
     if (const char *e = getenv("MHDGPU_XLINE_W")) {
         int w = atoi(e);
         if (w == 8 || w == 16 || w == 32) W = w;
     }
+    return xl_configure(c, W);
+}
+
+// Tiling, carries and tensor maps of the fused x pass for tile width W;
+// xf_W = 0 when the grid cannot be tiled (the steps then run through the
+// operator stage).
+static int xl_configure(Ctx *c, int W)
+{
+    int rc;
+    const long n = c->nx;
     while (W > 8 && W > c->ny) W /= 2;  // a tile never spans more columns than the grid
     const long rcap = xl_rcap(W);
     int C = (int)((n + rcap - 1) / rcap);
-    if (C > MHD_MAX_CLUSTER) return mhd_set_error(MHDGPU_ERR_UNSUPPORTED);
     long R = (n + C - 1) / C;
     if (W == 8 && (R % 2 || n % 2)) {  // 64-byte rows: copies must start on even rows
         W = 16;
@@ -826,6 +863,53 @@ int xline_setup(Ctx *c)
         return rc;
     if ((rc = xl_attrs<double>(C))) return rc;
     if ((rc = xl_attrs<float>(C))) return rc;
+    return MHDGPU_OK;
+}
+
+int fused_x_timing_pass(Ctx *c);
+
+// Time the fused x pass (its full program without a pending filter: the
+// state is only read) for each tile width the grid admits, keep the fastest
+// and remember it for this shape and precision.  *w_out: the width chosen.
+int xline_autotune(Ctx *c, int *w_out)
+{
+    if (c->xf_W == 0) return mhd_set_error(MHDGPU_ERR_UNSUPPORTED);
+    cudaEvent_t e0, e1;
+    MHD_CUDA_TRY(cudaEventCreate(&e0));
+    MHD_CUDA_TRY(cudaEventCreate(&e1));
+    int best = c->xf_W, rc = MHDGPU_OK;
+    float best_ms = 0.0f;
+    const int prev = c->xf_W;
+    for (int W : {8, 16, 32}) {
+        if (W > c->ny || (rc = xl_configure(c, W)) != MHDGPU_OK) break;
+        if (c->xf_W != W) continue;  // not admissible here
+        if ((rc = fused_x_timing_pass(c))) break;  // warm-up
+        cudaEventRecord(e0, c->stream);
+        for (int k = 0; k < 3 && !rc; k++) rc = fused_x_timing_pass(c);
+        cudaEventRecord(e1, c->stream);
+        if (rc || cudaEventSynchronize(e1) != cudaSuccess) {
+            rc = rc ? rc : mhd_set_error(MHDGPU_ERR_CUDA);
+            break;
+        }
+        float ms = 0.0f;
+        cudaEventElapsedTime(&ms, e0, e1);
+        if (best_ms == 0.0f || ms < best_ms) {
+            best_ms = ms;
+            best = W;
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (rc) {
+        xl_configure(c, prev);
+        return rc;
+    }
+    if ((rc = xl_configure(c, best))) return rc;
+    {
+        std::lock_guard<std::mutex> lock(g_xl_tuned_mu);
+        g_xl_tuned[XLTuneKey{c->nx, c->ny, c->nvar, c->mixed}] = c->xf_W;
+    }
+    if (w_out) *w_out = c->xf_W;
     return MHDGPU_OK;
 }
 

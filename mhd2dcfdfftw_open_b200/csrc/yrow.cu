@@ -35,6 +35,10 @@ struct YRArgs {
     int nvar;
     RhsCoef k;
     double cc, dd;
+    // device step control: with dtdev, cc = ccoef dt and dd = dcoef dt with
+    // dt = dtdev[0], and Ch, Cp = dtdev[1], dtdev[2] (hyperbolic cleaning)
+    const double *dtdev;
+    double ccoef, dcoef;
     int read_rk, write_rk;
     int d2u, d2b;  // second derivatives of u (viscosity) and B (resistivity or Hall)
     int *flag;     // status flag of bounded waits
@@ -190,6 +194,17 @@ __global__ void __launch_bounds__(YR_THREADS, (YRGeom<L, T>::MINB)) yrow_kernel(
 
     // ---- 2. right-hand side and RK3 update, point by point ------------------
     // (FP64 state and RK3 accumulation in both precisions; the fluxes in T)
+    double cc = a.cc, dd = a.dd;
+    RhsCoef kc = a.k;
+    if (a.dtdev) {
+        const double dt = a.dtdev[0];
+        cc = a.ccoef * dt;
+        dd = a.dcoef * dt;
+        if (kc.cleaning == 2) {
+            kc.Ch = a.dtdev[1];
+            kc.Cp = a.dtdev[2];
+        }
+    }
     if (valid) {
         const int nv = a.nvar;
         const T *dEdx = reinterpret_cast<const T *>(a.dEdx);
@@ -224,14 +239,14 @@ __global__ void __launch_bounds__(YR_THREADS, (YRGeom<L, T>::MINB)) yrow_kernel(
                 d2x[3 + c] = a.k.resist > 0 ? d2Bdx2[c * plane + o] : (T)0;
                 d2y[3 + c] = a.k.resist > 0 ? d2Bdy2[c * plane + o] : (T)0;
             }
-            rhs_point<T>(a.k, u, dx, dy, d2x, d2y, dEdx[plane + o], dEdx[2 * plane + o], dEdy[o],
+            rhs_point<T>(kc, u, dx, dy, d2x, d2y, dEdx[plane + o], dEdx[2 * plane + o], dEdy[o],
                          dEdy[2 * plane + o], (T)0, (T)0, r);
 #pragma unroll
             for (int v = 0; v < 9; v++) {
                 if (v < nv) {
                     double rk = a.read_rk ? a.dudtRK[v * plane + o] : 0.0;
                     const double rv = (double)r[v];
-                    a.uu[v * plane + o] = ud[v] + a.cc * rv + a.dd * rk;
+                    a.uu[v * plane + o] = ud[v] + cc * rv + dd * rk;
                     if (a.write_rk) a.dudtRK[v * plane + o] = rv;
                 }
             }
@@ -310,6 +325,11 @@ int launch_yrow(Ctx *c, int iRK, int last_stage)
                   p.divBcleaning};
     a.cc = c->cc[iRK];
     a.dd = c->dd[iRK];
+    static const double CC[3] = {8.0 / 15.0, 5.0 / 12.0, 0.75};  // rkInit, timeAdvance.c:20-27
+    static const double DD[3] = {0.0, -17. / 60., -5. / 12.};
+    a.dtdev = c->dev_dt ? c->dscal : nullptr;
+    a.ccoef = CC[iRK];
+    a.dcoef = DD[iRK];
     a.read_rk = iRK > 0;       // dd[0] = 0 and dudtRK is zero at the first stage
     a.write_rk = !last_stage;  // rkInit clears dudtRK after the last stage
     a.d2u = p.viscosity > 0;

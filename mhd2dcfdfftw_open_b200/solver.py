@@ -43,7 +43,7 @@ EXPORTED = (
     "mhdgpu_rk_execute", "mhdgpu_filtering", "mhdgpu_calc_dt", "mhdgpu_check_divb",
     "mhdgpu_get_cleaning_speeds", "mhdgpu_stage", "mhdgpu_steps", "mhdgpu_steps_fused",
     "mhdgpu_diagnostics", "mhdgpu_stream", "mhdgpu_launch_count", "mhdgpu_profile",
-    "mhdgpu_profile_read", "mhdgpu_set_precision",
+    "mhdgpu_profile_read", "mhdgpu_set_precision", "mhdgpu_autotune",
 )
 
 # arithmetic of the fused steps (mhdgpu_set_precision)
@@ -95,6 +95,7 @@ def load_library(path: str = LIB_PATH):
     L.mhdgpu_steps.argtypes = [vp, ctypes.c_int, ctypes.c_double, dp]
     L.mhdgpu_steps_fused.argtypes = [vp, ctypes.c_int, ctypes.c_double, dp]
     L.mhdgpu_set_precision.argtypes = [vp, ctypes.c_int]
+    L.mhdgpu_autotune.argtypes = [vp, ctypes.POINTER(ctypes.c_int)]
     L.mhdgpu_diagnostics.argtypes = [vp, dp, dp, ctypes.POINTER(ctypes.c_int)]
     L.mhdgpu_stream.argtypes = [vp]
     L.mhdgpu_stream.restype = vp
@@ -236,6 +237,14 @@ class Domain:
         RK3 accumulation)."""
         self._check(self.lib.mhdgpu_set_precision(
             self.h, PRECISION_MIXED if mixed else PRECISION_FP64))
+
+    def autotune(self):
+        """Pick the fastest tile width of the fused x pass for this grid and
+        precision (remembered for later domains of the same shape); returns
+        the width."""
+        w = ctypes.c_int(0)
+        self._check(self.lib.mhdgpu_autotune(self.h, ctypes.byref(w)))
+        return w.value
 
     def diagnostics(self):
         e, h, fin = ctypes.c_double(), ctypes.c_double(), ctypes.c_int()

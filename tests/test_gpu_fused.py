@@ -83,3 +83,50 @@ def test_fused_diffusive_cleaning_routes_to_operator_stage(reference):
         d.steps(2, 1e-3, fused=True)
         err = rel_l2(d.get("uu"), ru)
     assert err.max() < 1e-11, err
+
+
+def test_fused_cfl_steps_match_operator_steps():
+    # device step control (dt, Ch, Cp on the device, steps replayed as CUDA
+    # graphs) against the host-controlled operator path
+    p, uu = ic.orszag_tang(128, 64, di=0.05)
+    with Domain(p, uu) as a, Domain(p, uu) as b:
+        dta = a.steps(6, 0.0, dt=1e-3)
+        dtb = b.steps(6, 0.0, dt=1e-3, fused=True)
+        assert dtb == pytest.approx(dta, rel=1e-12)
+        assert rel_l2(b.get("uu"), a.get("uu")).max() < 1e-11
+
+
+@pytest.mark.parametrize("dt_fixed", [1e-3, 0.0])
+def test_graph_replay_equals_step_by_step(dt_fixed):
+    # one call of 6 steps (first eager, then the captured step replayed)
+    # against 6 calls of one step (all eager): the same launches, bit for bit
+    p, uu = ic.alfvenic_turbulence(256, 128, mmax=8)
+    with Domain(p, uu) as a, Domain(p, uu) as b:
+        dta = a.steps(6, dt_fixed, dt=2e-4, fused=True)
+        dtb = 2e-4
+        for _ in range(6):
+            dtb = b.steps(1, dt_fixed, dt=dtb, fused=True)
+        assert dta == dtb
+        np.testing.assert_array_equal(a.get("uu"), b.get("uu"))
+
+
+def test_hyperbolic_cleaning_fused_fixed_dt_vs_reference(reference):
+    p, uu = ic.orszag_tang(64, 64, di=0.05, divBcleaning=2)
+    ru, _ = run_ref(reference, p, uu, 5, 1e-3)
+    with Domain(p, uu) as d:
+        d.steps(5, 1e-3, fused=True)
+        err = rel_l2(d.get("uu"), ru)
+    assert err.max() < 1e-11, err
+
+
+@pytest.mark.parametrize("nx,ny", [(4096, 64), (256, 256)])
+def test_autotune_keeps_the_results(nx, ny):
+    # every tile width solves the same systems exactly: the tuned steps agree
+    # with the default ones to rounding
+    p, uu = ic.alfvenic_turbulence(nx, ny, mmax=8)
+    with Domain(p, uu) as a, Domain(p, uu) as b:
+        w = b.autotune()
+        assert w in (8, 16, 32)
+        a.steps(3, 2e-4, fused=True)
+        b.steps(3, 2e-4, fused=True)
+        assert rel_l2(b.get("uu"), a.get("uu")).max() < 1e-12

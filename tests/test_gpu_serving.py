@@ -43,7 +43,7 @@ def test_jobs_overlap_and_budget_holds():
     reqs = [S.Request(i, 256, 256, steps=60, kind="ot", mixed=True) for i in range(8)]
     budget = 4 * S.footprint_bytes(256, 256)
     res, wall = S.run_stream(reqs, budget_bytes=budget, slots=8, realtime=False)
-    assert all(r.error is None for r in res)
+    assert all(r.error is None for r in res), [r.error for r in res]
     # some job was admitted before another finished: the work overlapped
     spans = sorted((r.admitted, r.finished) for r in res)
     assert any(spans[i + 1][0] < spans[i][1] for i in range(len(spans) - 1))
