@@ -117,7 +117,33 @@ def cpu_processes():
     return max(1, min(n, 32))
 
 
-def run_reference_sample(nsteps, warmup, nproc, timeout=600):
+def workload(args, nx, ny):
+    """(params, state, dt, name) of the bench workload at nx x ny."""
+    from mhd2dcfdfftw_open_b200 import ic
+    if args.workload == "parametric":  # parametric decay of an Alfven pump, dt 5e-4
+        p, uu = ic.parametric_decay(nx, ny)
+        return p, uu, 5e-4, "parametric_decay"
+    p, uu = ic.alfvenic_turbulence(nx, ny)  # Alfvenic turbulence, dt 2e-4
+    return p, uu, DT, "alfvenic_turbulence"
+
+
+def arm_config(args, world):
+    """The `config` object both arms print for the same workload."""
+    cells = float(args.nx) * args.ny
+    name = "parametric_decay" if args.workload == "parametric" else "alfvenic_turbulence"
+    return {"workload": f"{name}_{args.nx}x{args.ny}_{'mixed' if args.precision == 'mixed' else 'fp64'}",
+            "nx": args.nx, "ny": args.ny, "precision": args.precision,
+            "dt": 5e-4 if args.workload == "parametric" else DT, "path": args.path,
+            "parallelism": f"replicas{world}",
+            "l2": f"inputs larger than L2 (state alone is {8 * cells * 8 / 1e9:.2f} GB)"}
+
+
+def data_label(args):
+    return ("synthetic (seeded parametric-decay IC, seed 3)" if args.workload == "parametric"
+            else "synthetic (seeded Alfvenic turbulence IC, seed 1)")
+
+
+def run_reference_sample(nsteps, warmup, nproc, timeout=600, args=None):
     """nproc concurrent single-rank reference processes, each running warmup +
     nsteps RK3 steps of the 1024^2 turbulence sample; returns
     (aggregate cell-updates/s, max seconds, per-process results)."""
@@ -129,12 +155,16 @@ def run_reference_sample(nsteps, warmup, nproc, timeout=600):
     if not os.path.exists(ref.BIN_PATH):
         raise RuntimeError("oracle/_ref/mhd_ref is not built")
     nx, ny = CPU_SAMPLE
-    p, uu = ic.alfvenic_turbulence(nx, ny)
+    if args is not None:
+        p, uu, dt, _ = workload(args, nx, ny)
+    else:
+        p, uu = ic.alfvenic_turbulence(nx, ny)
+        dt = DT
     with tempfile.TemporaryDirectory(prefix="mhdcpu_") as wd:
         p.write(os.path.join(wd, "input"))
         icp = os.path.join(wd, "ic.dat")
         write_state(icp, uu)
-        procs = [subprocess.Popen([ref.BIN_PATH, wd, icp, str(nsteps), repr(DT), "-", str(warmup)],
+        procs = [subprocess.Popen([ref.BIN_PATH, wd, icp, str(nsteps), repr(dt), "-", str(warmup)],
                                   stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
                  for _ in range(nproc)]
         res = []
@@ -207,12 +237,7 @@ def run_ours(args):
     from mhd2dcfdfftw_open_b200.solver import Domain
 
     nx, ny = args.nx, args.ny
-    if args.workload == "parametric":  # parametric decay of an Alfven pump, dt 5e-4
-        p, uu = ic.parametric_decay(nx, ny)
-        dt = 5e-4
-    else:                              # Alfvenic turbulence, dt 2e-4
-        p, uu = ic.alfvenic_turbulence(nx, ny)
-        dt = DT
+    p, uu, dt, _ = workload(args, nx, ny)
     fused = args.path == "fused"
     dom = Domain(p, uu, device=local)
     mixed = args.precision == "mixed"
@@ -313,14 +338,8 @@ def run_ours(args):
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f32 sweeps/FFT/fluxes, f64 state" if mixed else "f64",
-        "data": ("synthetic (seeded parametric-decay IC, seed 3)" if args.workload == "parametric"
-                 else "synthetic (seeded Alfvenic turbulence IC, seed 1)"),
-        "config": {"workload": f"{'parametric_decay' if args.workload == 'parametric' else 'alfvenic_turbulence'}"
-                               f"_{nx}x{ny}_{'mixed' if mixed else 'fp64'}",
-                   "nx": nx, "ny": ny, "precision": args.precision,
-                   "dt": dt, "path": args.path, "parallelism": f"replicas{world}",
-                   "l2": "inputs larger than L2 (state alone is "
-                         f"{8 * cells * 8 / 1e9:.2f} GB)"},
+        "data": data_label(args),
+        "config": arm_config(args, world),
         "roofline": roofline,
         "model_fraction": {"bytes_per_cell_update": algorithmic_model_bytes(),
                            "frac": round(value / world * algorithmic_model_bytes() / (peak * 1e9), 4)},
@@ -357,16 +376,16 @@ def run_reference(args):
     n = args.steps + args.warmup
     CPU_SAMPLE = (1024, 1024) if n <= 20 else ((512, 512) if n <= 80 else (256, 256))
     nproc = cpu_processes()
-    agg, tmax, _ = run_reference_sample(args.steps, args.warmup, nproc)
-    sample = (f"turbulence {CPU_SAMPLE[0]}x{CPU_SAMPLE[1]} per step, {nproc} independent "
-              "single-rank processes of the reference's C code (oracle/_ref/mhd_ref)")
+    agg, tmax, _ = run_reference_sample(args.steps, args.warmup, nproc, args=args)
+    sample = (f"{workload(args, 16, 16)[3]} {CPU_SAMPLE[0]}x{CPU_SAMPLE[1]} per step, {nproc} "
+              "independent single-rank processes of the reference's C code (oracle/_ref/mhd_ref), "
+              "FP64")
     out = {
         "metric": METRIC, "value": agg, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": tmax * 1e3 / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-        "data": "synthetic (seeded Alfvenic turbulence IC, seed 1)",
-        "config": {"workload": f"alfvenic_turbulence_{args.nx}x{args.ny}_fp64", "nx": args.nx,
-                   "ny": args.ny, "dt": DT, "sample": sample},
+        "data": data_label(args),
+        "config": arm_config(args, world),
         "impl": "reference",
         "cpu_baseline": {"value": agg, "unit": UNIT, "cores": nproc, "kind": "reference",
                          "sample": sample},

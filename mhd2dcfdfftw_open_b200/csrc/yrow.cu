@@ -219,16 +219,13 @@ __global__ void __launch_bounds__(YR_THREADS, (YRGeom<L, T>::MINB)) yrow_kernel(
         for (int m = 0; m < 16; m++) {
             const size_t o = ro + j + m * G::T_;
             T u[9], dx[9], dy[9], d2x[6], d2y[6], r[9];
-            double ud[9];
 #pragma unroll
             for (int v = 0; v < 9; v++) {
                 if (v < nv) {
-                    ud[v] = a.uu[v * plane + o];
-                    u[v] = (T)ud[v];
+                    u[v] = (T)a.uu[v * plane + o];
                     dx[v] = dudx[v * plane + o];
                     dy[v] = dudy[v * plane + o];
                 } else {
-                    ud[v] = 0.0;
                     u[v] = dx[v] = dy[v] = (T)0;
                 }
             }
@@ -246,7 +243,10 @@ __global__ void __launch_bounds__(YR_THREADS, (YRGeom<L, T>::MINB)) yrow_kernel(
                 if (v < nv) {
                     double rk = a.read_rk ? a.dudtRK[v * plane + o] : 0.0;
                     const double rv = (double)r[v];
-                    a.uu[v * plane + o] = ud[v] + cc * rv + dd * rk;
+                    // the FP64 state: re-read in FP32 mode (an L1 hit), the
+                    // value already held in FP64 mode
+                    const double ud = MIX ? a.uu[v * plane + o] : (double)u[v];
+                    a.uu[v * plane + o] = ud + cc * rv + dd * rk;
                     if (a.write_rk) a.dudtRK[v * plane + o] = rv;
                 }
             }

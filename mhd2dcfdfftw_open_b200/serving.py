@@ -30,7 +30,6 @@ from __future__ import annotations
 import argparse
 import dataclasses
 import json
-import math
 import threading
 import time
 
@@ -243,6 +242,7 @@ def main(argv=None):
     ap.add_argument("--rate", type=float, default=20.0)
     ap.add_argument("--slots", type=int, default=8)
     ap.add_argument("--budget-gb", type=float, default=150.0)
+    ap.add_argument("--steps-min", type=int, default=100)
     ap.add_argument("--steps-max", type=int, default=2000)
     ap.add_argument("--seed", type=int, default=5)
     ap.add_argument("--fp64", action="store_true", help="serve in FP64 instead of mixed")
@@ -254,14 +254,14 @@ def main(argv=None):
     sizes = ENSEMBLE_SIZES if a.ensemble else SERVING_SIZES
     rate = 0.0 if a.ensemble else a.rate
     reqs = draw_requests(a.requests, a.seed, rate, sizes, not a.ensemble,
-                         (100, a.steps_max), mixed=not a.fp64)
+                         (a.steps_min, a.steps_max), mixed=not a.fp64)
     res, wall = run_stream(reqs, a.budget_gb * 1e9, a.slots, realtime=rate > 0)
     out = {"workload": "ensemble" if a.ensemble else "serving", "requests": a.requests,
            "rate_per_s": rate, "slots": a.slots, "precision": "fp64" if a.fp64 else "mixed",
            "served": summarize(res, wall)}
     if a.baseline:
         base = draw_requests(a.requests, a.seed, rate, sizes, not a.ensemble,
-                             (100, a.steps_max), mixed=False)
+                             (a.steps_min, a.steps_max), mixed=False)
         bres, bwall = run_stream(base, a.budget_gb * 1e9, 1, realtime=rate > 0)
         out["baseline_fp64_one_at_a_time"] = summarize(bres, bwall)
     print(json.dumps(out), flush=True)
