@@ -419,7 +419,9 @@ __device__ void xl_solve(const XFArgs &a, const XLSmem<T> &s, cg::cluster_group 
             }
         }
     }
-    __syncthreads();  // everyone has read preE/preP before the scan rewrites them
+    // Each thread has read its own preE/preP above; the scan that rewrites
+    // them runs only after the barrier below, which every thread reaches
+    // after that read, so the backward aggregates need no barrier before.
 #pragma unroll
     for (int r = 0; r < NR; r++) s.aggE[r][ai] = xv[r];
     s.aggP[ai] = Q;

@@ -25,6 +25,7 @@ constexpr int YR_THREADS = 256;
 
 struct YRArgs {
     double *uu, *dudtRK;
+    double *spec;  // the context's dudt array: per-row scratch of d2/dy2 spectra
     // derivative arrays: doubles, or floats (field v at v * nx * ny) in the
     // mixed-precision stage
     const void *dudx, *d2udx2, *d2Bdx2, *dEdx;
@@ -121,6 +122,60 @@ __device__ __forceinline__ void yr_op(const typename YRCplx<T>::C *tw, typename 
     __syncthreads();  // A may be refilled
 }
 
+// d/dy and d2/dy2 of one pair from one forward FFT: the d2/dy2 spectrum is
+// parked in global scratch (element i < N/2 at lo[i], the others at hi[i];
+// each thread parks and takes back its own elements, so no barrier guards
+// it) while the d/dy inverse runs in A.
+template <int L, typename T>
+__device__ __forceinline__ void yr_op12(const typename YRCplx<T>::C *tw, typename YRCplx<T>::C *A,
+                                        int j, bool valid, const typename YRCplx<T>::C *s1,
+                                        const typename YRCplx<T>::C *s2,
+                                        typename YRCplx<T>::C *lo, typename YRCplx<T>::C *hi,
+                                        T *o1a, T *o1b, T *o2a, T *o2b)
+{
+    using G = YRGeom<L, T>;
+    using C = typename G::C;
+    __syncthreads();  // the row is complete
+    fft_row<L, -1>(A, tw, j);
+#pragma unroll
+    for (int m = 0; m < 16; m++) {
+        const int i = j + m * G::T_;
+        const C z = A[fpad(i)];
+        // i < N/2 exactly when m < 8; rows past the grid park nothing
+        if (valid) (m < 8 ? lo : hi)[i] = cm(z, __ldg(s2 + i));
+        A[fpad(i)] = cm(z, __ldg(s1 + i));
+    }
+    __syncthreads();
+    fft_row<L, +1>(A, tw, j);
+    if (valid) {
+#pragma unroll
+        for (int m = 0; m < 16; m++) {
+            const int i = j + m * G::T_;
+            const C z = A[fpad(i)];
+            if (o1a) o1a[i] = z.x;
+            if (o1b) o1b[i] = z.y;
+        }
+    }
+    __syncthreads();  // every thread has read its d/dy values
+#pragma unroll
+    for (int m = 0; m < 16; m++) {
+        const int i = j + m * G::T_;
+        A[fpad(i)] = valid ? (m < 8 ? lo : hi)[i] : cmk<C>((T)0, (T)0);
+    }
+    __syncthreads();
+    fft_row<L, +1>(A, tw, j);
+    if (valid) {
+#pragma unroll
+        for (int m = 0; m < 16; m++) {
+            const int i = j + m * G::T_;
+            const C z = A[fpad(i)];
+            if (o2a) o2a[i] = z.x;
+            if (o2b) o2b[i] = z.y;
+        }
+    }
+    __syncthreads();  // A may be refilled
+}
+
 template <int L, typename T>
 __global__ void __launch_bounds__(YR_THREADS, (YRGeom<L, T>::MINB)) yrow_kernel(YRArgs a)
 {
@@ -158,8 +213,6 @@ __global__ void __launch_bounds__(YR_THREADS, (YRGeom<L, T>::MINB)) yrow_kernel(
         const int fb = q == 0 ? UY : q == 1 ? P : q == 2 ? BZ : q == 3 ? BY : -1;
         const double *ra = su(fa), *rb = fb >= 0 ? su(fb) : nullptr;
         const double ca = sh(ra), cb = rb ? sh(rb) : 0.0;
-        yr_load<L, T>(A, ra, rb, ca, cb, j, valid);
-        yr_op<L, T, false>(tw, A, j, valid, s1, f(a.dudy, fa), fb >= 0 ? f(a.dudy, fb) : nullptr);
         T *o2a = nullptr, *o2b = nullptr;
         if (fa == UX && a.d2u) { o2a = f(a.d2udy2, 0); o2b = f(a.d2udy2, 1); }
         if (fa == UZ) {
@@ -167,9 +220,19 @@ __global__ void __launch_bounds__(YR_THREADS, (YRGeom<L, T>::MINB)) yrow_kernel(
             o2b = a.d2b ? f(a.d2Bdy2, 2) : nullptr;
         }
         if (fa == BX && a.d2b) { o2a = f(a.d2Bdy2, 0); o2b = f(a.d2Bdy2, 1); }
+        yr_load<L, T>(A, ra, rb, ca, cb, j, valid);
         if (o2a || o2b) {  // uniform across the block
-            yr_load<L, T>(A, ra, rb, ca, cb, j, valid);
-            yr_op<L, T, false>(tw, A, j, valid, s2, o2a, o2b);
+            // this row's slots of the scratch array: a row of field 2q holds
+            // N/2 double2 (FP64: the second half goes to field 2q + 1) or N
+            // float2 (FP32)
+            C *lo = reinterpret_cast<C *>(a.spec + (size_t)(2 * q) * plane + ro);
+            C *hi = sizeof(C) == 16
+                        ? reinterpret_cast<C *>(a.spec + (size_t)(2 * q + 1) * plane + ro) - G::N / 2
+                        : lo;
+            yr_op12<L, T>(tw, A, j, valid, s1, s2, lo, hi, f(a.dudy, fa),
+                          fb >= 0 ? f(a.dudy, fb) : nullptr, o2a, o2b);
+        } else {
+            yr_op<L, T, false>(tw, A, j, valid, s1, f(a.dudy, fa), fb >= 0 ? f(a.dudy, fb) : nullptr);
         }
     }
     {   // (Ex, Ez) = (uz By - uy Bz, uy Bx - ux By), formed in FP64
@@ -302,6 +365,7 @@ int launch_yrow(Ctx *c, int iRK, int last_stage)
     YRArgs a;
     a.uu = c->arr[MHDGPU_UU];
     a.dudtRK = c->arr[MHDGPU_DUDTRK];
+    a.spec = c->arr[MHDGPU_DUDT];  // unused by the fused stage otherwise
     a.dudx = c->arr[MHDGPU_DUDX];
     a.d2udx2 = c->arr[MHDGPU_D2UDX2];
     a.d2Bdx2 = c->arr[MHDGPU_D2BDX2];
