@@ -132,7 +132,8 @@ int mhdgpu_set_precision(mhdgpu_ctx *ctx, int precision);
  * pass for each tile width this grid admits (8, 16, 32 columns per CTA; the
  * rows per CTA and the cluster size follow from it) at the context's current
  * precision, keeps the fastest and remembers it for contexts of the same
- * shape and precision created later in this process.  The state is only
+ * shape created later in this process (a shape already tuned in this
+ * process keeps its width, so runs repeat bit for bit).  The state is only
  * read; the derivative arrays are overwritten.  *columns_out: the width
  * chosen (may be NULL).  MHDGPU_ERR_UNSUPPORTED when the grid has no fused x
  * pass. */

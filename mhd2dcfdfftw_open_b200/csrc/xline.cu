@@ -744,14 +744,14 @@ static int xl_attrs(int C)
     return MHDGPU_OK;
 }
 
-// Tile widths picked by xline_autotune, per grid shape and precision, for
-// the contexts this process creates later.
+// Tile widths picked by xline_autotune, per grid shape, for the contexts
+// this process creates later.
 struct XLTuneKey {
     long nx, ny;
-    int nvar, mixed;
+    int nvar;
     bool operator<(const XLTuneKey &o) const
     {
-        return std::tie(nx, ny, nvar, mixed) < std::tie(o.nx, o.ny, o.nvar, o.mixed);
+        return std::tie(nx, ny, nvar) < std::tie(o.nx, o.ny, o.nvar);
     }
 };
 static std::map<XLTuneKey, int> g_xl_tuned;
@@ -773,7 +773,7 @@ int xline_setup(Ctx *c)
     int W = n <= XLGeom<32>::RCAP ? 32 : 8;
     {
         std::lock_guard<std::mutex> lock(g_xl_tuned_mu);
-        auto it = g_xl_tuned.find(XLTuneKey{c->nx, c->ny, c->nvar, c->mixed});
+        auto it = g_xl_tuned.find(XLTuneKey{c->nx, c->ny, c->nvar});
         if (it != g_xl_tuned.end()) W = it->second;
     }
     if (const char *e = getenv("MHDGPU_XLINE_W")) {
@@ -871,11 +871,26 @@ static int xl_configure(Ctx *c, int W)
 int fused_x_timing_pass(Ctx *c);
 
 // Time the fused x pass (its full program without a pending filter: the
-// state is only read) for each tile width the grid admits, keep the fastest
-// and remember it for this shape and precision.  *w_out: the width chosen.
+// state is only read) at the context's precision for each tile width the
+// grid admits, keep the fastest and remember it for this shape.  *w_out: the
+// width chosen.
 int xline_autotune(Ctx *c, int *w_out)
 {
     if (c->xf_W == 0) return mhd_set_error(MHDGPU_ERR_UNSUPPORTED);
+    {   // a shape tuned before in this process keeps its width (runs repeat bit for bit)
+        int known = 0;
+        {
+            std::lock_guard<std::mutex> lock(g_xl_tuned_mu);
+            auto it = g_xl_tuned.find(XLTuneKey{c->nx, c->ny, c->nvar});
+            if (it != g_xl_tuned.end()) known = it->second;
+        }
+        if (known) {
+            int rc = known == c->xf_W ? MHDGPU_OK : xl_configure(c, known);
+            if (rc) return rc;
+            if (w_out) *w_out = c->xf_W;
+            return MHDGPU_OK;
+        }
+    }
     cudaEvent_t e0, e1;
     MHD_CUDA_TRY(cudaEventCreate(&e0));
     MHD_CUDA_TRY(cudaEventCreate(&e1));
@@ -909,7 +924,7 @@ int xline_autotune(Ctx *c, int *w_out)
     if ((rc = xl_configure(c, best))) return rc;
     {
         std::lock_guard<std::mutex> lock(g_xl_tuned_mu);
-        g_xl_tuned[XLTuneKey{c->nx, c->ny, c->nvar, c->mixed}] = c->xf_W;
+        g_xl_tuned[XLTuneKey{c->nx, c->ny, c->nvar}] = c->xf_W;
     }
     if (w_out) *w_out = c->xf_W;
     return MHDGPU_OK;

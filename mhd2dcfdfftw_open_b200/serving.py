@@ -109,6 +109,7 @@ class Server:
         self._stop = False
         self._t0 = None
         self.results: list[Result] = []
+        self._tuned: set = set()  # grid shapes whose x-pass tiling has been autotuned
         self._workers = [threading.Thread(target=self._work, daemon=True) for _ in range(slots)]
         for w in self._workers:
             w.start()
@@ -160,6 +161,12 @@ class Server:
         try:
             with Domain(p, uu, device=self.device) as d:
                 d.set_precision(req.mixed)
+                shape = (req.nx, req.ny)
+                with self._cv:
+                    tune = shape not in self._tuned
+                    self._tuned.add(shape)
+                if tune:  # the first job of a shape picks the tiling for the later ones
+                    d.autotune()
                 dt = req.dt0
                 left = req.steps
                 while left > 0:
