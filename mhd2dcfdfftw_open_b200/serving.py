@@ -190,10 +190,47 @@ class Server:
             w.join()
 
 
-def run_stream(requests, budget_bytes=150e9, slots=8, device=0, realtime=True):
-    """Feed `requests` to a Server at their arrival times (realtime) or all at
-    once; return (results, wall seconds)."""
-    srv = Server(budget_bytes, slots, device)
+class Router:
+    """Several GPUs of one node: one Server per device, each request placed
+    whole on the device with the fewest bytes placed so far plus reserved
+    now (ties to the lower device).  Jobs never span devices, so no
+    collective is involved; results are gathered on the host."""
+
+    def __init__(self, devices, budget_bytes: float = 150e9, slots: int = 8,
+                 server_cls=None):
+        cls = server_cls or Server
+        self.servers = [cls(budget_bytes, slots, d) for d in devices]
+        self._lock = threading.Lock()
+        self._placed = [0.0] * len(self.servers)  # footprint bytes placed so far
+        self.placement: dict = {}
+
+    def start_clock(self):
+        for s in self.servers:
+            s.start_clock()
+
+    def clock(self) -> float:
+        return self.servers[0].clock()
+
+    def submit(self, req: Request):
+        fp = footprint_bytes(req.nx, req.ny)
+        with self._lock:
+            k = min(range(len(self.servers)),
+                    key=lambda i: (self._placed[i] + self.servers[i]._reserved, i))
+            self._placed[k] += fp
+            self.placement[req.rid] = self.servers[k].device
+        self.servers[k].submit(req)
+
+    def drain(self):
+        for s in self.servers:
+            s.drain()
+        return [r for s in self.servers for r in s.results]
+
+
+def run_stream(requests, budget_bytes=150e9, slots=8, device=0, realtime=True, devices=None):
+    """Feed `requests` to a Server (or, with `devices`, a Router over those
+    GPUs) at their arrival times (realtime) or all at once; return (results,
+    wall seconds)."""
+    srv = Router(devices, budget_bytes, slots) if devices else Server(budget_bytes, slots, device)
     srv.start_clock()
     for r in sorted(requests, key=lambda q: q.arrival):
         if realtime:
@@ -203,9 +240,9 @@ def run_stream(requests, budget_bytes=150e9, slots=8, device=0, realtime=True):
         else:
             r.arrival = srv.clock()
         srv.submit(r)
-    srv.drain()
-    wall = max(x.finished for x in srv.results) if srv.results else 0.0
-    return sorted(srv.results, key=lambda x: x.rid), wall
+    results = srv.drain() if devices else (srv.drain() or srv.results)
+    wall = max(x.finished for x in results) if results else 0.0
+    return sorted(results, key=lambda x: x.rid), wall
 
 
 def summarize(results, wall):
@@ -248,6 +285,7 @@ def main(argv=None):
     ap.add_argument("--requests", type=int, default=200)
     ap.add_argument("--rate", type=float, default=20.0)
     ap.add_argument("--slots", type=int, default=8)
+    ap.add_argument("--gpus", type=int, default=1, help="route jobs over this many GPUs")
     ap.add_argument("--budget-gb", type=float, default=150.0)
     ap.add_argument("--steps-min", type=int, default=100)
     ap.add_argument("--steps-max", type=int, default=2000)
@@ -262,7 +300,8 @@ def main(argv=None):
     rate = 0.0 if a.ensemble else a.rate
     reqs = draw_requests(a.requests, a.seed, rate, sizes, not a.ensemble,
                          (a.steps_min, a.steps_max), mixed=not a.fp64)
-    res, wall = run_stream(reqs, a.budget_gb * 1e9, a.slots, realtime=rate > 0)
+    res, wall = run_stream(reqs, a.budget_gb * 1e9, a.slots, realtime=rate > 0,
+                           devices=list(range(a.gpus)) if a.gpus > 1 else None)
     out = {"workload": "ensemble" if a.ensemble else "serving", "requests": a.requests,
            "rate_per_s": rate, "slots": a.slots, "precision": "fp64" if a.fp64 else "mixed",
            "served": summarize(res, wall)}

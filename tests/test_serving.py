@@ -87,3 +87,29 @@ def test_summary_percentiles():
     assert s["p50_latency_s"] == np.percentile(np.arange(1, 101), 50)
     assert s["p99_latency_s"] == np.percentile(np.arange(1, 101), 99)
     assert s["cell_updates_per_s"] == 100 * 100 * 10 / 100.0
+
+
+def test_router_places_whole_jobs_across_devices():
+    reqs = S.draw_requests(60, seed=9, rate=0.0, sizes=S.ENSEMBLE_SIZES,
+                           inverse_cells=False, steps=(100, 200))
+    budget = 2 * S.footprint_bytes(1024, 1024)
+    r = S.Router([0, 1], budget, slots=3, server_cls=FakeServer)
+    r.start_clock()
+    for q in reqs:
+        r.submit(q)
+    res = r.drain()
+    assert sorted(x.rid for x in res) == list(range(60))   # every job ran exactly once
+    assert set(r.placement.values()) == {0, 1}            # both devices used
+    for srv in r.servers:
+        assert srv.peak_bytes <= budget                    # each device keeps its budget
+    work = [sum(S.footprint_bytes(q.nx, q.ny) for q in reqs if r.placement[q.rid] == d)
+            for d in (0, 1)]
+    assert max(work) < 2.0 * min(work)                     # roughly balanced by bytes
+
+
+def test_run_stream_over_a_router(monkeypatch):
+    monkeypatch.setattr(S, "Server", FakeServer)
+    reqs = S.draw_requests(12, seed=2, rate=0.0, sizes=((128, 128), (256, 256)),
+                           inverse_cells=False, steps=(100, 100))
+    res, wall = S.run_stream(reqs, budget_bytes=1e12, slots=2, realtime=False, devices=[0, 1])
+    assert [r.rid for r in res] == list(range(12)) and wall > 0
