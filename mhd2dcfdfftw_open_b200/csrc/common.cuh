@@ -86,10 +86,7 @@ struct Ctx {
     double cc[3], dd[3];
     double Ch, Cp;
     double dt;
-    // fused path scratch
-    double *fx[16];              // x-pass outputs of the fused stage
-    double *yscr;                // per-CTA row scratch of the fused y pass
-    long yscr_rows;
+    // fused path
     int fused_pending_filter;    // 1: uu still needs the x filter
     // instrumentation: launch counter and per-kernel-class event timing
     long launches;

@@ -23,7 +23,6 @@ struct XFTables {
 struct XFArgs {
     const double *in;     // source array (field 0)
     int in_start;         // first source field
-    int src_kind;         // 0 field, 1 Ey, 2 Ez (from in = uu)
     double *fout;         // filtered-field output (field-indexed), or null: no filter
     double *out1;         // first-derivative output (field-indexed), or null
     double *out2a;        // second-derivative output for fields [d2a_lo, d2a_lo+3)
