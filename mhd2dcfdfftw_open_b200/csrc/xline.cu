@@ -433,6 +433,19 @@ __device__ void xl_solve(const XFArgs &a, const XLSmem<T> &s, cg::cluster_group 
     T cb[NR];
     xl_inflow<W, NR, T>(a, cluster, cta, crank, 1, lane, cb);
     const T pQ = s.preP[ai];
+    // The filtered line's boundary rows also go straight into the halo rows
+    // of the neighbouring CTAs' tiles (periodic: the first and last CTA are
+    // neighbours).  The neighbours read their halos only in their forward
+    // sweeps, which they finished before the cluster barriers above.
+    double *hp = nullptr, *hn = nullptr;  // prv's right halo, nxt's left halo (row 0, this lane)
+    if constexpr (NR == 1 && OP0 == XOP_F) {
+        if (tout) {
+            const int C = a.C, prv = (crank - 1 + C) % C, nxt = (crank + 1) % C;
+            const int Rp = (int)min((long)a.R, nx - (long)prv * a.R);
+            hp = cluster.map_shared_rank(tout, prv) + (Rp + XL_H) * W + lane;
+            hn = cluster.map_shared_rank(tout, nxt) + lane;
+        }
+    }
 #pragma unroll
     for (int r = 0; r < NR; r++) {
         T d = s.preE[r][ai] + pQ * cb[r];
@@ -449,7 +462,11 @@ __device__ void xl_solve(const XFArgs &a, const XLSmem<T> &s, cg::cluster_group 
                 else v = (OT)x;
                 if (g) g[(size_t)l * ny] = v;
                 if constexpr (NR == 1 && OP0 == XOP_F) {
-                    if (tout) tout[(l + XL_H) * W + lane] = (double)v;
+                    if (tout) {
+                        tout[(l + XL_H) * W + lane] = (double)v;
+                        if (l < XL_H) hp[l * W] = (double)v;
+                        if (l >= Rc - XL_H) hn[(l - (Rc - XL_H)) * W] = (double)v;
+                    }
                 }
             }
         }
@@ -597,20 +614,9 @@ xline_kernel(XFArgs a, const __grid_constant__ CUtensorMap tm_big,
             double *g = col ? a.fout + (size_t)v * plane + j0 + lane : nullptr;
             xl_solve<W, XOP_F, XOP_F, 1, T>(a, s, cluster, t, t, g, nullptr, t, Rc, r0, crank, par);
             par ^= 1;
-            cluster.sync();  // every CTA's tile holds its filtered core rows
-            // halo rows of the filtered line from the neighbouring CTAs
-            const int prv = (crank - 1 + C) % C, nxt = (crank + 1) % C;
-            const int Rp = (int)min((long)a.R, nx - (long)prv * a.R);
-            const double *tp = cluster.map_shared_rank(t, prv);
-            const double *tn = cluster.map_shared_rank(t, nxt);
-            if (tid < XL_H * W) {  // own halo rows: no other CTA reads them
-                int r = tid / W, cc = tid % W;
-                t[r * W + cc] = tp[(Rp + r) * W + cc];
-            } else if (tid < 2 * XL_H * W) {
-                int r = (tid - XL_H * W) / W, cc = tid % W;
-                t[(Rc + XL_H + r) * W + cc] = tn[(XL_H + r) * W + cc];
-            }
-            __syncthreads();
+            // every CTA's tile holds its filtered core rows and, pushed by
+            // its neighbours, the filtered halo rows
+            cluster.sync();
         }
         if (!a.out1) continue;
         T *g1 = col ? o1 + (size_t)v * plane + j0 + lane : nullptr;
