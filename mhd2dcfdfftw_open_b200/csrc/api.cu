@@ -460,10 +460,6 @@ extern "C" int mhdgpu_steps(mhdgpu_ctx *h, int nsteps, double dt_fixed, double *
     return check_flag(c);
 }
 
-// Steps through the fused stage (fused.cu).  Diffusive cleaning
-// (divBcleaning == 1) needs d/dx, d/dy of divB inside the stage, and grids the
-// fused x pass cannot tile (an odd nx with 8 columns), run through the
-// operator stage instead.
 // One fused RK3 step under device step control: the three fused stages and,
 // with CFL control or hyperbolic cleaning, the x filter they leave pending
 // and calcDt for the next step, all on the device.
@@ -477,10 +473,9 @@ static int fused_step_dev(Ctx *c, bool need_dt, bool keep_dt)
     return MHDGPU_OK;
 }
 
-// Steps through the fused stage (fused.cu).  Diffusive cleaning
-// (divBcleaning == 1) needs d/dx, d/dy of divB inside the stage, and grids the
-// fused x pass cannot tile (an odd nx with 8 columns), run through the
-// operator stage instead.
+// Steps through the fused stage (fused.cu).  Grids the fused x pass cannot
+// tile (an odd nx with 8 columns), and diffusive cleaning (divBcleaning == 1)
+// where the y row kernel does not apply, run through the operator stage.
 //
 // With the row kernel (16 <= ny <= 4096) the step control stays on the
 // device: dt (and Ch, Cp) live in dscal, the y pass forms cc = c_k dt and
@@ -497,7 +492,8 @@ extern "C" int mhdgpu_steps_fused(mhdgpu_ctx *h, int nsteps, double dt_fixed, do
     if (nsteps < 0) return mhd_set_error(MHDGPU_ERR_INVALID);
     if (c->mixed && (c->p.divBcleaning == 1 || c->xf_W == 0 || !mhd::yrow_supported(c)))
         return mhd_set_error(MHDGPU_ERR_UNSUPPORTED);
-    if (c->p.divBcleaning == 1 || c->xf_W == 0) return mhdgpu_steps(h, nsteps, dt_fixed, dt_io);
+    if (c->xf_W == 0 || (c->p.divBcleaning == 1 && !mhd::yrow_supported(c)))
+        return mhdgpu_steps(h, nsteps, dt_fixed, dt_io);
     if (nsteps > 0) c->deriv_fp32 = c->mixed;
     const bool need_dt = dt_fixed <= 0 || c->p.divBcleaning == 2;
     double dt = dt_io ? *dt_io : 0.0;

@@ -94,14 +94,26 @@ int fused_apply_pending_filter(Ctx *c)
 }
 
 bool yrow_supported(const Ctx *c);
-int launch_yrow(Ctx *c, int iRK, int last_stage);
+int launch_yrow(Ctx *c, int iRK, int last_stage, int mode);
 
 int fused_stage(Ctx *c, int iRK, int first, int last)
 {
     (void)first;
     int rc = fused_x_pass(c);
     if (rc) return rc;
-    rc = yrow_supported(c) ? launch_yrow(c, iRK, last) : fused_y_pass(c, iRK);
+    if (c->p.divBcleaning == 1 && yrow_supported(c)) {
+        // diffusive cleaning (mhd.c:175-182): divB needs both passes'
+        // derivatives, and its own derivatives the whole lines: the y pass
+        // splits around calcDivB and the two operator derivatives of divB
+        double *divb = c->arr[MHDGPU_DIVB];
+        if ((rc = launch_yrow(c, iRK, last, 1))) return rc;
+        if ((rc = launch_divb(c, divb))) return rc;
+        if ((rc = launch_xsolve(c, XOP_D1, 1, divb, 0, c->arr[MHDGPU_DDIVBDX], 0))) return rc;
+        if ((rc = launch_yspec(c, 0, 1, divb, 0, c->arr[MHDGPU_DDIVBDY], 0))) return rc;
+        rc = launch_yrow(c, iRK, last, 2);
+    } else {
+        rc = yrow_supported(c) ? launch_yrow(c, iRK, last, 0) : fused_y_pass(c, iRK);
+    }
     if (rc) return rc;
     c->fused_pending_filter = 1;
     return MHDGPU_OK;

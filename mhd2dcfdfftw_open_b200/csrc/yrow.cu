@@ -40,6 +40,10 @@ struct YRArgs {
     // dt = dtdev[0], and Ch, Cp = dtdev[1], dtdev[2] (hyperbolic cleaning)
     const double *dtdev;
     double ccoef, dcoef;
+    // 0: the whole y pass; 1: its y derivatives only; 2: the rest (RHS,
+    // RK3, filter), with d(divB)/dx, d(divB)/dy read for diffusive cleaning
+    int mode;
+    const double *ddivbdx, *ddivbdy;
     int read_rk, write_rk;
     int d2u, d2b;  // second derivatives of u (viscosity) and B (resistivity or Hall)
     int *flag;     // status flag of bounded waits
@@ -208,7 +212,7 @@ __global__ void __launch_bounds__(YR_THREADS, (YRGeom<L, T>::MINB)) yrow_kernel(
     // d/dy of every field, d2/dy2 of u and B (a second forward FFT of the
     // pair, reloaded from L2, instead of keeping the spectrum)
     const int npair = a.nvar == 9 ? 5 : 4;
-    for (int q = 0; q < npair; q++) {
+    for (int q = 0; q < (a.mode == 2 ? 0 : npair); q++) {
         const int fa = q == 0 ? UX : q == 1 ? RHO : q == 2 ? UZ : q == 3 ? BX : PSI;
         const int fb = q == 0 ? UY : q == 1 ? P : q == 2 ? BZ : q == 3 ? BY : -1;
         const double *ra = su(fa), *rb = fb >= 0 ? su(fb) : nullptr;
@@ -235,7 +239,7 @@ __global__ void __launch_bounds__(YR_THREADS, (YRGeom<L, T>::MINB)) yrow_kernel(
             yr_op<L, T, false>(tw, A, j, valid, s1, f(a.dudy, fa), fb >= 0 ? f(a.dudy, fb) : nullptr);
         }
     }
-    {   // (Ex, Ez) = (uz By - uy Bz, uy Bx - ux By), formed in FP64
+    if (a.mode != 2) {  // (Ex, Ez) = (uz By - uy Bz, uy Bx - ux By), formed in FP64
         auto efield = [&](size_t o, double &ex, double &ez) {
             const double *u = a.uu + o;
             double ux = u[UX * plane], uy = u[UY * plane], uz = u[UZ * plane];
@@ -254,6 +258,8 @@ __global__ void __launch_bounds__(YR_THREADS, (YRGeom<L, T>::MINB)) yrow_kernel(
         }
         yr_op<L, T, false>(tw, A, j, valid, s1, f(a.dEdy, 0), f(a.dEdy, 2));
     }
+
+    if (a.mode == 1) return;  // uniform across the grid
 
     // ---- 2. right-hand side and RK3 update, point by point ------------------
     // (FP64 state and RK3 accumulation in both precisions; the fluxes in T)
@@ -299,8 +305,10 @@ __global__ void __launch_bounds__(YR_THREADS, (YRGeom<L, T>::MINB)) yrow_kernel(
                 d2x[3 + c] = a.k.resist > 0 ? d2Bdx2[c * plane + o] : (T)0;
                 d2y[3 + c] = a.k.resist > 0 ? d2Bdy2[c * plane + o] : (T)0;
             }
+            const T dbx = a.ddivbdx ? (T)a.ddivbdx[o] : (T)0;
+            const T dby = a.ddivbdy ? (T)a.ddivbdy[o] : (T)0;
             rhs_point<T>(kc, u, dx, dy, d2x, d2y, dEdx[plane + o], dEdx[2 * plane + o], dEdy[o],
-                         dEdy[2 * plane + o], (T)0, (T)0, r);
+                         dEdy[2 * plane + o], dbx, dby, r);
 #pragma unroll
             for (int v = 0; v < 9; v++) {
                 if (v < nv) {
@@ -359,7 +367,7 @@ static int launch_yrow_l(Ctx *c, const YRArgs &a, double bytes)
 // Whether the row kernel serves this context (16 <= ny <= 4096).
 bool yrow_supported(const Ctx *c) { return c->ny >= 16 && c->ny <= 4096; }
 
-int launch_yrow(Ctx *c, int iRK, int last_stage)
+int launch_yrow(Ctx *c, int iRK, int last_stage, int mode)
 {
     const mhdgpu_params &p = c->p;
     YRArgs a;
@@ -394,6 +402,10 @@ int launch_yrow(Ctx *c, int iRK, int last_stage)
     a.dtdev = c->dev_dt ? c->dscal : nullptr;
     a.ccoef = CC[iRK];
     a.dcoef = DD[iRK];
+    a.mode = mode;
+    const bool diffuse = p.divBcleaning == 1;
+    a.ddivbdx = diffuse ? c->arr[MHDGPU_DDIVBDX] : nullptr;
+    a.ddivbdy = diffuse ? c->arr[MHDGPU_DDIVBDY] : nullptr;
     a.read_rk = iRK > 0;       // dd[0] = 0 and dudtRK is zero at the first stage
     a.write_rk = !last_stage;  // rkInit clears dudtRK after the last stage
     a.d2u = p.viscosity > 0;

@@ -130,3 +130,22 @@ def test_autotune_keeps_the_results(nx, ny):
         a.steps(3, 2e-4, fused=True)
         b.steps(3, 2e-4, fused=True)
         assert rel_l2(b.get("uu"), a.get("uu")).max() < 1e-12
+
+
+def test_diffusive_cleaning_fused_vs_reference(reference):
+    # divBcleaning = 1: the y pass splits around calcDivB and the operator
+    # derivatives of divB (mhd.c:175-182)
+    p, uu = ic.orszag_tang(64, 64, di=0.05, divBcleaning=1)
+    ru, _ = run_ref(reference, p, uu, 5, 1e-3)
+    with Domain(p, uu) as d:
+        d.steps(5, 1e-3, fused=True)
+        err = rel_l2(d.get("uu"), ru)
+    assert err.max() < 1e-11, err
+
+
+def test_diffusive_cleaning_fused_matches_operator_path_long_lines():
+    p, uu = ic.orszag_tang(4096, 64, di=0.05, divBcleaning=1)
+    with Domain(p, uu) as a, Domain(p, uu) as b:
+        a.steps(3, 1e-4)
+        b.steps(3, 1e-4, fused=True)
+        assert rel_l2(b.get("uu"), a.get("uu")).max() < 1e-12
