@@ -10,8 +10,11 @@
 // at the state (the end of a run, a CFL time step, a host read).
 //
 //   x pass:  per field, F_x (if pending) -> write state -> d/dx, d2/dx2
-//            (xfused.cu); then d/dx of Ey, Ez with E computed from the state.
-//   y pass:  d/dy, d2/dy2, E, calcRHS, rkExecute, F_y.
+//            (xline.cu); then d/dx of Ey, Ez with E computed from the state.
+//   y pass:  d/dy, d2/dy2, E, calcRHS, rkExecute, F_y (yrow.cu; with
+//            diffusive cleaning split around calcDivB and the divB
+//            derivatives; for rows the row kernel does not take, the
+//            operator kernels in the same order).
 #include <cstring>
 
 #include "common.cuh"

@@ -1,5 +1,5 @@
 // Device helpers shared by the x-direction line kernels (xsolve.cu,
-// xfused.cu): the compact-scheme right-hand sides of mathlib.c:46-85,
+// xline.cu): the compact-scheme right-hand sides of mathlib.c:46-85,
 // 176-217 and 309-353, TMA bulk copies with mbarrier completion, and bounded
 // waits.
 #pragma once

@@ -9,20 +9,24 @@
 // Layout of the work.  A cluster of C CTAs owns W adjacent columns over the
 // whole line and walks all fields of that column tile:
 //   * field v+1 is staged into the second of two shared-memory tiles by the
-//     TMA engine (cp.async.bulk, one W*8-byte copy per row, mbarrier
-//     completion) while field v is solved;
+//     TMA engine (2-D tensor-map boxes of W columns, mbarrier completion)
+//     while field v is solved;
 //   * 512 threads per CTA, two CTAs per SM (one CTA's barrier waits overlap
 //     the other's sweeps): thread (column, sub-chunk) keeps its 8 rows of a
 //     recurrence in registers; the exact inflows of each sub-chunk come from
 //     a warp-shuffle scan of the sub-chunk (end value, product) pairs inside
-//     the CTA and of the CTA pairs across the cluster, read through
-//     distributed shared memory;
-//   * the filtered line replaces the tile's core rows and its three halo rows
-//     on each side are copied from the neighbouring CTAs' tiles, so the line
-//     is read from HBM once for all three operators.
+//     the CTA and of the totals of at most two neighbouring CTAs, read
+//     through distributed shared memory;
+//   * d/dx and d2/dx2 of a field, and dEy/dx with dEz/dx, share their matrix
+//     and run as one paired solve;
+//   * the filtered line replaces the tile's core rows, and each CTA pushes its
+//     first and last filtered rows into its neighbours' halo rows, so the
+//     line is read from HBM once for all three operators.
 // Rows away from the two line ends use the constant interior Thomas factors
 // and a branch-free interior stencil; the few sub-chunks that touch the first
 // or last XF_EDGE rows use the tabulated factors and the closure stencils.
+// T is the type of the recurrences: double, or float in mixed precision
+// (where the filter is solved for its change; see xl_solve).
 #include <cooperative_groups.h>
 
 #include <cudaTypedefs.h>
