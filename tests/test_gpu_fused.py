@@ -149,3 +149,26 @@ def test_diffusive_cleaning_fused_matches_operator_path_long_lines():
         a.steps(3, 1e-4)
         b.steps(3, 1e-4, fused=True)
         assert rel_l2(b.get("uu"), a.get("uu")).max() < 1e-12
+
+
+@pytest.mark.parametrize("mixed", [False, True])
+def test_checkpoint_restart_is_exact(tmp_path, mixed):
+    # a job paused at a step boundary (state written in the reference's
+    # out%04d.dat format, writeOutput.c) and resumed in a new context gives the
+    # same fields bit for bit: dudtRK is reset every step, so uu is the state
+    from mhd2dcfdfftw_open_b200 import dumpio
+    p, uu = ic.alfvenic_turbulence(256, 128, mmax=8)
+    with Domain(p, uu) as a:
+        a.set_precision(mixed)
+        a.steps(10, 2e-4, fused=True)
+        full = a.get("uu")
+    with Domain(p, uu) as b:
+        b.set_precision(mixed)
+        b.steps(5, 2e-4, fused=True)
+        dumpio.write_state(str(tmp_path / "out0001.dat"), b.get("uu"), 5 * 2e-4)
+    t, saved = dumpio.read_state(str(tmp_path / "out0001.dat"), p.nvar, p.nx, p.ny)
+    assert t == pytest.approx(1e-3)
+    with Domain(p, saved) as c:
+        c.set_precision(mixed)
+        c.steps(5, 2e-4, fused=True)
+        np.testing.assert_array_equal(c.get("uu"), full)
