@@ -20,7 +20,7 @@ sizes from a list (probability proportional to 1/cells for serving), the
 Orszag-Tang or the turbulence generator by seed parity, d_i ~ U[0, 0.1],
 eta = nu ~ logU[1e-4, 1e-3], Hall = 1, CFL 0.3, Poisson arrivals.
 
-    python -m mhd2dcfdfftw_open_b200.serving --requests 200 --rate 20 --slots 8
+    python -m mhd2dcfdfftw_open_b200.serving --requests 200 --rate 20 --slots 32
 
 prints one JSON line: p50/p99 completion latency, sustained cell-updates/s,
 and the same stream run plain FP64 one job at a time (--baseline).
@@ -292,7 +292,7 @@ def main(argv=None):
     ap = argparse.ArgumentParser(description=__doc__.split("\n\n")[0])
     ap.add_argument("--requests", type=int, default=200)
     ap.add_argument("--rate", type=float, default=20.0)
-    ap.add_argument("--slots", type=int, default=8)
+    ap.add_argument("--slots", type=int, default=32)
     ap.add_argument("--gpus", type=int, default=1, help="route jobs over this many GPUs")
     ap.add_argument("--budget-gb", type=float, default=150.0)
     ap.add_argument("--steps-min", type=int, default=100)
