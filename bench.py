@@ -313,7 +313,10 @@ def run_ours(args):
             if den < 1e-8 * float(np.linalg.norm(ref)):
                 den = float(np.linalg.norm(ref))
             per.append(float(np.linalg.norm(mix[v] - ref[v]) / den))
+        tot = float(np.linalg.norm(ref))
+        per_state = [float(np.linalg.norm(mix[v] - ref[v]) / tot) for v in range(ref.shape[0])]
         mixed_error = {"rel_l2_per_field": per, "rel_l2_max": max(per),
+                       "l2_vs_state_norm_per_field": per_state,
                        "steps": args.warmup + args.steps,
                        "against": "FP64 fused steps on the GPU (which match the reference to 1e-12)"}
 
