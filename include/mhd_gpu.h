@@ -168,6 +168,12 @@ int mhdgpu_calc_dt_noalloc(const double *d_uu, const mhdgpu_params *p, double dt
 void *mhdgpu_stream(mhdgpu_ctx *ctx);
 /* number of kernels this context has launched so far */
 long mhdgpu_launch_count(const mhdgpu_ctx *ctx);
+/* Self-test of the bounded waits (no counterpart in the reference): runs a
+ * kernel whose mbarrier wait is never satisfied, with a limit of
+ * `milliseconds` (0 < ms <= 2000).  Returns MHDGPU_ERR_TIMEOUT, read from the
+ * context's status flag exactly as a stalled TMA copy in the x kernels would
+ * be reported; the flag is cleared and the context stays usable. */
+int mhdgpu_selftest_wait(mhdgpu_ctx *ctx, double milliseconds);
 /* enable (1) / disable (0) CUDA-event bracketing of every launch; enabling
  * clears the record */
 int mhdgpu_profile(mhdgpu_ctx *ctx, int enable);

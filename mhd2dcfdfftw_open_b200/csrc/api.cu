@@ -262,7 +262,11 @@ extern "C" int mhdgpu_get_array(mhdgpu_ctx *h, int which, double *host)
     return MHDGPU_OK;
 }
 
-static int check_flag(Ctx *c)
+int mhd_check_flag(Ctx *c);
+static int check_flag(Ctx *c) { return mhd_check_flag(c); }
+
+// status flag of the context's kernels: read, report and clear
+int mhd_check_flag(Ctx *c)
 {
     int f = 0;
     MHD_CUDA_TRY(cudaMemcpyAsync(&f, c->dflag, sizeof(int), cudaMemcpyDeviceToHost, c->stream));

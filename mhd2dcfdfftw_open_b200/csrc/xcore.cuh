@@ -109,14 +109,15 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, unsigned parity)
     return ok != 0;
 }
 
-// Bounded wait on an mbarrier phase: about 2 s of SM clocks at most, then the
-// error flag is raised and the caller carries on (the data are then garbage,
-// which the host reports as MHDGPU_ERR_TIMEOUT).
-__device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, unsigned parity, int *flag)
+// Bounded wait on an mbarrier phase: `limit` SM clocks at most (about 2 s by
+// default), then the error flag is raised and the caller carries on (the data
+// are then garbage, which the host reports as MHDGPU_ERR_TIMEOUT).
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, unsigned parity, int *flag,
+                                                  long long limit = 4000000000LL)
 {
     long long t0 = clock64();
     while (!mbar_try_wait(bar, parity)) {
-        if (clock64() - t0 > 4000000000LL) {
+        if (clock64() - t0 > limit) {
             if (flag) atomicExch(flag, MHDGPU_ERR_TIMEOUT);
             return false;
         }

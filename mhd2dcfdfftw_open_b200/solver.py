@@ -43,7 +43,7 @@ EXPORTED = (
     "mhdgpu_rk_execute", "mhdgpu_filtering", "mhdgpu_calc_dt", "mhdgpu_check_divb",
     "mhdgpu_get_cleaning_speeds", "mhdgpu_stage", "mhdgpu_steps", "mhdgpu_steps_fused",
     "mhdgpu_diagnostics", "mhdgpu_stream", "mhdgpu_launch_count", "mhdgpu_profile",
-    "mhdgpu_profile_read", "mhdgpu_set_precision", "mhdgpu_autotune",
+    "mhdgpu_profile_read", "mhdgpu_set_precision", "mhdgpu_autotune", "mhdgpu_selftest_wait",
 )
 
 # arithmetic of the fused steps (mhdgpu_set_precision)
@@ -96,6 +96,7 @@ def load_library(path: str = LIB_PATH):
     L.mhdgpu_steps_fused.argtypes = [vp, ctypes.c_int, ctypes.c_double, dp]
     L.mhdgpu_set_precision.argtypes = [vp, ctypes.c_int]
     L.mhdgpu_autotune.argtypes = [vp, ctypes.POINTER(ctypes.c_int)]
+    L.mhdgpu_selftest_wait.argtypes = [vp, ctypes.c_double]
     L.mhdgpu_diagnostics.argtypes = [vp, dp, dp, ctypes.POINTER(ctypes.c_int)]
     L.mhdgpu_stream.argtypes = [vp]
     L.mhdgpu_stream.restype = vp
