@@ -166,13 +166,26 @@ class Server:
                     n = left if self.chunk <= 0 else min(left, self.chunk)
                     dt = d.steps(n, req.dt_fixed, dt=dt, fused=True)
                     left -= n
-                e = d.diagnostics()["energy"]
+                diag = d.diagnostics()
                 out = d.get("uu") if req.keep_state else None
+            # a state that left the finite numbers is this job's error, not the server's
+            err = None if diag["finite"] else "non-finite state (NaN or Inf) at the end of the job"
             return Result(req.rid, req.nx * req.ny, req.steps, req.arrival, admitted,
-                          self.clock(), dt, e, out)
+                          self.clock(), dt, diag["energy"], out, err)
         except Exception as exc:  # reported per job, the server keeps serving
             return Result(req.rid, req.nx * req.ny, req.steps, req.arrival, admitted,
                           self.clock(), 0.0, float("nan"), None, str(exc))
+
+    def cancel(self, rid: int) -> bool:
+        """Withdraw a request that has not been admitted yet; False when it
+        is running, finished or unknown."""
+        with self._cv:
+            for i, q in enumerate(self._queue):
+                if q.rid == rid:
+                    self._queue.pop(i)
+                    self._cv.notify_all()
+                    return True
+        return False
 
     def drain(self):
         """Wait for every submitted job, then stop the workers."""

@@ -54,3 +54,26 @@ def test_jobs_overlap_and_budget_holds():
         live += d
         peak = max(peak, live)
     assert peak <= 4
+
+
+def test_poisoned_job_fails_alone():
+    # host-side fault injection: one job starts from a state with a NaN; it is
+    # reported as that job's error and the others are unaffected
+    jobs = _jobs(False)
+    bad = S.Request(99, 128, 128, steps=20, kind="ot", keep_state=True)
+    orig = bad.build
+
+    def poisoned():
+        p, uu = orig()
+        uu = uu.copy()
+        uu[0, 5, 7] = np.nan
+        return p, uu
+
+    bad.build = poisoned
+    res, _ = S.run_stream(jobs + [bad], slots=6, realtime=False)
+    byid = {r.rid: r for r in res}
+    assert byid[99].error is not None and "non-finite" in byid[99].error
+    alone, _ = S.run_stream(_jobs(False), slots=1, realtime=False)
+    for a in alone:
+        assert byid[a.rid].error is None
+        np.testing.assert_array_equal(byid[a.rid].uu, a.uu)

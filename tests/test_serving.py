@@ -113,3 +113,15 @@ def test_run_stream_over_a_router(monkeypatch):
                            inverse_cells=False, steps=(100, 100))
     res, wall = S.run_stream(reqs, budget_bytes=1e12, slots=2, realtime=False, devices=[0, 1])
     assert [r.rid for r in res] == list(range(12)) and wall > 0
+
+
+def test_queued_request_can_be_cancelled():
+    srv = FakeServer(S.footprint_bytes(256, 256), slots=1)
+    srv.start_clock()
+    reqs = [S.Request(i, 256, 256, steps=2000) for i in range(4)]   # the first runs ~40 ms
+    for r in reqs:
+        srv.submit(r)
+    assert srv.cancel(3) is True          # still queued behind the budget
+    assert srv.cancel(99) is False        # unknown
+    srv.drain()
+    assert sorted(r.rid for r in srv.results) == [0, 1, 2]
