@@ -89,10 +89,21 @@ class Result:
     energy: float
     uu: np.ndarray | None = None
     error: str | None = None
+    cross_helicity: float = float("nan")
 
     @property
     def latency(self) -> float:
         return self.finished - self.arrival
+
+    def record(self) -> dict:
+        """The job's JSON record: size, steps, time step, energy and cross
+        helicity at the end, latency, and its own cell-updates/s while admitted."""
+        busy = self.finished - self.admitted
+        return {"rid": self.rid, "cells": self.cells, "steps": self.steps, "dt": self.dt,
+                "energy": self.energy, "cross_helicity": self.cross_helicity,
+                "latency_s": self.latency, "queued_s": self.admitted - self.arrival,
+                "cell_updates_per_s": self.cells * self.steps / busy if busy > 0 else None,
+                "error": self.error}
 
 
 class Server:
@@ -171,7 +182,7 @@ class Server:
             # a state that left the finite numbers is this job's error, not the server's
             err = None if diag["finite"] else "non-finite state (NaN or Inf) at the end of the job"
             return Result(req.rid, req.nx * req.ny, req.steps, req.arrival, admitted,
-                          self.clock(), dt, diag["energy"], out, err)
+                          self.clock(), dt, diag["energy"], out, err, diag["cross_helicity"])
         except Exception as exc:  # reported per job, the server keeps serving
             return Result(req.rid, req.nx * req.ny, req.steps, req.arrival, admitted,
                           self.clock(), 0.0, float("nan"), None, str(exc))
@@ -316,6 +327,7 @@ def main(argv=None):
                     help="ensemble sizes, uniform, all submitted at once")
     ap.add_argument("--baseline", action="store_true",
                     help="also run the same stream plain FP64, one job at a time")
+    ap.add_argument("--records", default="", help="write one JSON record per job to this file")
     a = ap.parse_args(argv)
     sizes = ENSEMBLE_SIZES if a.ensemble else SERVING_SIZES
     rate = 0.0 if a.ensemble else a.rate
@@ -325,6 +337,10 @@ def main(argv=None):
         pretune(reqs, dev)  # the served stream and the baseline share the tiling
     res, wall = run_stream(reqs, a.budget_gb * 1e9, a.slots, realtime=rate > 0,
                            devices=list(range(a.gpus)) if a.gpus > 1 else None)
+    if a.records:
+        with open(a.records, "w") as f:
+            for r in res:
+                f.write(json.dumps(r.record()) + "\n")
     out = {"workload": "ensemble" if a.ensemble else "serving", "requests": a.requests,
            "rate_per_s": rate, "slots": a.slots, "precision": "fp64" if a.fp64 else "mixed",
            "served": summarize(res, wall)}

@@ -125,3 +125,11 @@ def test_queued_request_can_be_cancelled():
     assert srv.cancel(99) is False        # unknown
     srv.drain()
     assert sorted(r.rid for r in srv.results) == [0, 1, 2]
+
+
+def test_job_record_fields():
+    r = S.Result(3, 128 * 128, 100, 1.0, 2.0, 4.0, 1e-3, 0.5, None, None, 0.1)
+    rec = r.record()
+    assert rec["latency_s"] == 3.0 and rec["queued_s"] == 1.0
+    assert rec["cell_updates_per_s"] == 128 * 128 * 100 / 2.0
+    assert rec["cross_helicity"] == 0.1 and rec["error"] is None
