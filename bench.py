@@ -15,9 +15,10 @@ replica of the domain (the whole domain lives on one GPU: replicas only, no
 collective on the data path); the timing is the max over ranks.
 
 `--impl reference` times the reference's own C implementation of the path
-(compiled from its sources into oracle/_ref/mhd_ref) on the host cores:
-P independent single-rank processes, each step a bounded sample (1024 x 1024
-turbulence, one RK3 step per process).
+(compiled from its sources into oracle/_ref/mhd_ref) on the host cores, on the
+same grid: P concurrent independent single-rank processes (P = min(cores,
+--steps, what host memory holds at ~8.6 GB per 4096^2 process)), each timing
+one RK3 step of the full grid; the same sample is the GPU arm's cpu_baseline.
 """
 from __future__ import annotations
 
@@ -107,14 +108,37 @@ class ClockSampler:
 
 
 # ---------------------------------------------------------------------------
-# the reference's CPU path (oracle/_ref/mhd_ref), bounded samples
+# the reference's CPU path (oracle/_ref/mhd_ref) on the bench workload itself
 # ---------------------------------------------------------------------------
-CPU_SAMPLE = (1024, 1024)
+def host_mem_available():
+    """MemAvailable of /proc/meminfo in bytes (None where unreadable)."""
+    try:
+        with open("/proc/meminfo") as f:
+            for line in f:
+                if line.startswith("MemAvailable:"):
+                    return int(line.split()[1]) * 1024
+    except OSError:
+        pass
+    return None
 
 
-def cpu_processes():
+def ref_process_bytes(nx, ny):
+    """Host bytes of one single-rank reference process on an nx x ny grid:
+    about 62 field-sized arrays (initialize.c:216-320 with eta, nu > 0) plus
+    the state it reads, rounded up to 64 fields."""
+    return 64 * nx * ny * 8 + (nx * ny * 8 * 8)
+
+
+def cpu_processes(nx, ny, want=None):
+    """Concurrent reference processes: one per host core, at most `want`,
+    and no more than 75 % of the available host memory holds."""
     n = os.cpu_count() or 1
-    return max(1, min(n, 32))
+    if want is not None:
+        n = min(n, want)
+    mem = host_mem_available()
+    if mem is not None:
+        n = min(n, int(0.75 * mem // ref_process_bytes(nx, ny)))
+    return max(1, n)
 
 
 def workload(args, nx, ny):
@@ -127,10 +151,70 @@ def workload(args, nx, ny):
     return p, uu, DT, "alfvenic_turbulence"
 
 
+def run_reference_sample(args, nproc, nsteps=1, timeout=1800):
+    """`nproc` concurrent single-rank processes of the reference's C code,
+    each on the bench workload's full nx x ny grid from the same initial
+    state: set-up and state load untimed, then `nsteps` timed RK3 steps,
+    started together (a go file releases every process once all are ready).
+    Returns (aggregate cell-updates/s, slowest process's seconds, results)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import ref  # the checker's build of the reference (test infrastructure)
+    from mhd2dcfdfftw_open_b200.dumpio import write_state
+
+    if not os.path.exists(ref.BIN_PATH):
+        raise RuntimeError("oracle/_ref/mhd_ref is not built")
+    nx, ny = args.nx, args.ny
+    p, uu, dt, _ = workload(args, nx, ny)
+    with tempfile.TemporaryDirectory(prefix="mhdcpu_") as wd:
+        p.write(os.path.join(wd, "input"))
+        icp = os.path.join(wd, "ic.dat")
+        write_state(icp, uu)
+        del uu
+        go = os.path.join(wd, "go")
+        procs = [subprocess.Popen([ref.BIN_PATH, wd, icp, str(nsteps), repr(dt), "-", "0", go],
+                                  stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+                 for _ in range(nproc)]
+        try:
+            t_end = time.time() + timeout
+            for pr in procs:  # every process has set up and loaded the state
+                while True:  # the reference prints a banner of its own first
+                    line = pr.stdout.readline()
+                    if not line or time.time() > t_end:
+                        raise RuntimeError("a reference process did not get ready")
+                    if line.strip() == "READY":
+                        break
+            open(go, "w").close()
+            res = []
+            for pr in procs:
+                out, _ = pr.communicate(timeout=max(1.0, t_end - time.time()))
+                line = [ln for ln in out.splitlines() if ln.startswith("{")][-1]
+                res.append(json.loads(line))
+        finally:
+            for pr in procs:
+                if pr.poll() is None:
+                    pr.kill()
+    tmax = max(r["seconds"] for r in res)
+    agg = nproc * nx * ny * nsteps / tmax
+    return agg, tmax, res
+
+
+def reference_sample_text(args, nproc, tmax, nsteps=1):
+    name = workload_name(args)
+    return (f"{name} {args.nx}x{args.ny} (the full bench grid), {nsteps} RK3 step in each of "
+            f"{nproc} concurrent independent single-rank processes of the reference's C code "
+            f"(oracle/_ref/mhd_ref), started together; slowest process {tmax:.1f} s per step; "
+            f"set-up untimed; no warm-up step, the stage arrays' pages written once before "
+            f"timing instead (a first step's page faults excluded); FP64")
+
+
+def workload_name(args):
+    return "parametric_decay" if args.workload == "parametric" else "alfvenic_turbulence"
+
+
 def arm_config(args, world):
     """The `config` object both arms print for the same workload."""
     cells = float(args.nx) * args.ny
-    name = "parametric_decay" if args.workload == "parametric" else "alfvenic_turbulence"
+    name = workload_name(args)
     return {"workload": f"{name}_{args.nx}x{args.ny}_{'mixed' if args.precision == 'mixed' else 'fp64'}",
             "nx": args.nx, "ny": args.ny, "precision": args.precision,
             "dt": 5e-4 if args.workload == "parametric" else DT, "path": args.path,
@@ -141,40 +225,6 @@ def arm_config(args, world):
 def data_label(args):
     return ("synthetic (seeded parametric-decay IC, seed 3)" if args.workload == "parametric"
             else "synthetic (seeded Alfvenic turbulence IC, seed 1)")
-
-
-def run_reference_sample(nsteps, warmup, nproc, timeout=600, args=None):
-    """nproc concurrent single-rank reference processes, each running warmup +
-    nsteps RK3 steps of the 1024^2 turbulence sample; returns
-    (aggregate cell-updates/s, max seconds, per-process results)."""
-    sys.path.insert(0, os.path.join(ROOT, "oracle"))
-    import ref  # the checker's build of the reference (test infrastructure)
-    from mhd2dcfdfftw_open_b200 import ic
-    from mhd2dcfdfftw_open_b200.dumpio import write_state
-
-    if not os.path.exists(ref.BIN_PATH):
-        raise RuntimeError("oracle/_ref/mhd_ref is not built")
-    nx, ny = CPU_SAMPLE
-    if args is not None:
-        p, uu, dt, _ = workload(args, nx, ny)
-    else:
-        p, uu = ic.alfvenic_turbulence(nx, ny)
-        dt = DT
-    with tempfile.TemporaryDirectory(prefix="mhdcpu_") as wd:
-        p.write(os.path.join(wd, "input"))
-        icp = os.path.join(wd, "ic.dat")
-        write_state(icp, uu)
-        procs = [subprocess.Popen([ref.BIN_PATH, wd, icp, str(nsteps), repr(dt), "-", str(warmup)],
-                                  stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
-                 for _ in range(nproc)]
-        res = []
-        for pr in procs:
-            out, _ = pr.communicate(timeout=timeout)
-            line = [ln for ln in out.splitlines() if ln.startswith("{")][-1]
-            res.append(json.loads(line))
-    tmax = max(r["seconds"] for r in res)
-    agg = nproc * nx * ny * nsteps / tmax
-    return agg, tmax, res
 
 
 # ---------------------------------------------------------------------------
@@ -355,12 +405,10 @@ def run_ours(args):
     }
     if world == 1 and not args.no_cpu_baseline:
         try:
-            nproc = cpu_processes()
-            agg, tmax, _ = run_reference_sample(1, 0, nproc)
+            nproc = cpu_processes(nx, ny, want=args.cpu_procs)
+            agg, tmax, _ = run_reference_sample(args, nproc)
             out["cpu_baseline"] = {"value": agg, "unit": UNIT, "cores": nproc, "kind": "reference",
-                                   "sample": f"turbulence {CPU_SAMPLE[0]}x{CPU_SAMPLE[1]}, 1 RK3 step "
-                                             f"in each of {nproc} independent single-rank "
-                                             f"processes ({tmax:.1f} s)"}
+                                   "sample": reference_sample_text(args, nproc, tmax)}
         except Exception as e:  # reported, not hidden
             out["cpu_baseline"] = {"value": None, "error": str(e)[:200]}
     print(json.dumps(out), flush=True)
@@ -372,26 +420,26 @@ def run_ours(args):
 # reference arm
 # ---------------------------------------------------------------------------
 def run_reference(args):
+    """The reference's CPU implementation of the path on the bench workload's
+    own grid: min(cores, --steps, memory) concurrent processes, one timed RK3
+    step of the full grid each (the --steps requested full-grid steps would
+    take about a minute each on one core)."""
     rank, _, world = env_rank()
     if rank != 0:
         return
-    global CPU_SAMPLE
-    n = args.steps + args.warmup
-    CPU_SAMPLE = (1024, 1024) if n <= 20 else ((512, 512) if n <= 80 else (256, 256))
-    nproc = cpu_processes()
-    agg, tmax, _ = run_reference_sample(args.steps, args.warmup, nproc, args=args)
-    sample = (f"{workload(args, 16, 16)[3]} {CPU_SAMPLE[0]}x{CPU_SAMPLE[1]} per step, {nproc} "
-              "independent single-rank processes of the reference's C code (oracle/_ref/mhd_ref), "
-              "FP64")
+    nproc = cpu_processes(args.nx, args.ny, want=min(args.steps, args.cpu_procs or 1 << 30))
+    agg, tmax, _ = run_reference_sample(args, nproc)
     out = {
         "metric": METRIC, "value": agg, "unit": UNIT, "n_gpus": world, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": tmax * 1e3 / args.steps,
+        "warmup": args.warmup, "ms_per_step": tmax * 1e3,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": data_label(args),
         "config": arm_config(args, world),
         "impl": "reference",
+        "timed": {"processes": nproc, "steps_per_process": 1, "warmup_steps": 0,
+                  "grid": [args.nx, args.ny], "same_config": True},
         "cpu_baseline": {"value": agg, "unit": UNIT, "cores": nproc, "kind": "reference",
-                         "sample": sample},
+                         "sample": reference_sample_text(args, nproc, tmax)},
         "e2e": {"value": agg, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(out), flush=True)
@@ -410,6 +458,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--precision", choices=["fp64", "mixed"], default="fp64")
     ap.add_argument("--workload", choices=["turbulence", "parametric"], default="turbulence")
+    ap.add_argument("--cpu-procs", type=int, default=None,
+                    help="at most this many concurrent reference processes on the host")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

@@ -158,7 +158,10 @@ int mhdgpu_diagnostics(mhdgpu_ctx *ctx, double *energy, double *cross_helicity,
  * grids return MHDGPU_ERR_INVALID.  Calls share that array: calls that
  * overlap on the GPU race and must be serialised by the caller.  The first
  * call on a device looks the array up with that device current; make it
- * before any stream capture begins. */
+ * before any stream capture begins.  A NaN in the state does not make the
+ * result NaN (fmin and fmax drop NaN operands), as in mhdgpu_calc_dt; the
+ * reference's loop returns NaN only when its very first cell is NaN.  Use
+ * mhdgpu_diagnostics to detect a non-finite state. */
 int mhdgpu_calc_dt_noalloc(const double *d_uu, const mhdgpu_params *p, double dt0,
                            double *d_out, void *stream);
 

@@ -73,12 +73,14 @@ def build(force: bool = False, verbose: bool = False) -> str:
     return LIB
 
 
-def build_dropin_demo(ref_dir: str = "/root/reference") -> None:
+def build_dropin_demo(ref_dir: str | None = None) -> None:
     """Link the reference's own driver against the drop-in layer (needs the
-    reference sources; outputs go to oracle/_ref/)."""
+    reference sources: `ref_dir`, else $MHD_REF_DIR, else the default of
+    oracle/Makefile; outputs go to oracle/_ref/)."""
     build()
-    subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle"), f"REF_DIR={ref_dir}",
-                    "dropin"], check=True)
+    d = ref_dir or os.environ.get("MHD_REF_DIR")
+    cmd = ["make", "-s", "-C", os.path.join(ROOT, "oracle")] + ([f"REF_DIR={d}"] if d else [])
+    subprocess.run(cmd + ["dropin"], check=True)
 
 
 if __name__ == "__main__":

@@ -32,7 +32,7 @@ extern double *divB, *ddivBdx, *ddivBdy, *Efield, *dEdx, *dEdy, *dudt, *dudtRK;
 extern double *uuHaloX0, *uuHaloX1, *divBHaloX0, *divBHaloX1, *EfieldHaloX0, *EfieldHaloX1;
 
 static mhdgpu_ctx *g_ctx = NULL;
-static size_t g_nx = 0, g_ny = 0;
+static mhdgpu_params g_p;  /* the parameters g_ctx was created with */
 static int g_reported = 0;
 
 static void report(const char *where, int rc)
@@ -43,12 +43,21 @@ static void report(const char *where, int rc)
     }
 }
 
-/* the context, created from the globals initialize() has set */
+static int same_params(const mhdgpu_params *a, const mhdgpu_params *b)
+{
+    return a->boundaryTypeX == b->boundaryTypeX && a->cfl == b->cfl && a->Tmax == b->Tmax &&
+           a->dtOut == b->dtOut && a->nx == b->nx && a->ny == b->ny && a->Lx == b->Lx &&
+           a->Ly == b->Ly && a->adiabaticIdx == b->adiabaticIdx && a->Hall == b->Hall &&
+           a->di == b->di && a->resistivity == b->resistivity && a->viscosity == b->viscosity &&
+           a->divBcleaning == b->divBcleaning && a->outDivB == b->outDivB;
+}
+
+/* the context, created from the globals initialize() has set; a caller that
+ * changes any of them between calls gets a context made for the new values */
 static mhdgpu_ctx *ctx(void)
 {
-    if (g_ctx && g_nx == nx && g_ny == ny) return g_ctx;
-    if (g_ctx) mhdgpu_destroy(g_ctx);
     mhdgpu_params p;
+    memset(&p, 0, sizeof p);
     p.boundaryTypeX = boundaryTypeX;
     p.cfl = cfl;
     p.Tmax = Tmax;
@@ -64,6 +73,9 @@ static mhdgpu_ctx *ctx(void)
     p.viscosity = viscosity;
     p.divBcleaning = divBcleaning;
     p.outDivB = outDivB;
+    if (g_ctx && same_params(&p, &g_p)) return g_ctx;
+    if (g_ctx) mhdgpu_destroy(g_ctx);
+    g_ctx = NULL;
     const char *dev = getenv("MHDGPU_DEVICE");
     int rc = mhdgpu_create(&p, dev ? atoi(dev) : 0, &g_ctx);
     if (rc != MHDGPU_OK) {
@@ -71,8 +83,7 @@ static mhdgpu_ctx *ctx(void)
         g_ctx = NULL;
         return NULL;
     }
-    g_nx = nx;
-    g_ny = ny;
+    g_p = p;
     return g_ctx;
 }
 

@@ -19,7 +19,10 @@
 //    it and must be serialised by the caller;
 //  - the first call on a device looks up the array's device address
 //    (cudaGetSymbolAddress) with that device current; make that first call
-//    before any stream capture begins.
+//    before any stream capture begins;
+//  - fmin and fmax drop NaN operands, so a NaN in the state does not make
+//    the result NaN, exactly as in the context's calcDt (pointwise.cu); the
+//    reference's loop returns NaN only when its very first cell is NaN.
 #include <mutex>
 
 #include "common.cuh"

@@ -14,6 +14,8 @@
 // are served from L2; the updated state is written by step 2 and read back
 // (again from L2) and overwritten by step 3.  One padded FFT row per CTA row
 // and at most 128 registers per thread keep two CTAs on each SM.
+#include <mutex>
+
 #include "common.cuh"
 #include "fft.cuh"
 #include "rhscore.cuh"
@@ -347,14 +349,20 @@ static int launch_yrow_l(Ctx *c, const YRArgs &a, double bytes)
 {
     using G = YRGeom<L, T>;
     const size_t smem = G::SMEM;
-    static bool attr_done[64] = {false};  // per device
+    // the shared-memory attribute, set once per device; contexts on several
+    // host threads launch here concurrently
+    static std::mutex attr_mu;
+    static bool attr_done[64] = {false};
     int dev = 0;
     MHD_CUDA_TRY(cudaGetDevice(&dev));
     if (dev < 0 || dev >= 64) return mhd_set_error(MHDGPU_ERR_UNSUPPORTED);
-    if (!attr_done[dev]) {
-        MHD_CUDA_TRY(cudaFuncSetAttribute(yrow_kernel<L, T>,
-                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        attr_done[dev] = true;
+    {
+        std::lock_guard<std::mutex> lock(attr_mu);
+        if (!attr_done[dev]) {
+            MHD_CUDA_TRY(cudaFuncSetAttribute(yrow_kernel<L, T>,
+                                              cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+            attr_done[dev] = true;
+        }
     }
     const unsigned grid = (unsigned)((c->nx + G::ROWS - 1) / G::ROWS);
     prof_begin(c, KC_FUSED_Y, bytes);

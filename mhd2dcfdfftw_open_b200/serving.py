@@ -160,15 +160,24 @@ class Server:
             if req is None:
                 return
             admitted = self.clock()
-            res = self._run(req, admitted)
-            with self._cv:
-                self._reserved -= fp
-                self.results.append(res)
-                self._cv.notify_all()
+            res = None
+            try:
+                res = self._run(req, admitted)
+            finally:
+                # the reservation is returned whatever happened to the job,
+                # so a queued head request can always be admitted later
+                with self._cv:
+                    self._reserved -= fp
+                    if res is None:
+                        res = Result(req.rid, req.nx * req.ny, req.steps, req.arrival, admitted,
+                                     self.clock(), 0.0, float("nan"), None,
+                                     "worker failed before recording a result")
+                    self.results.append(res)
+                    self._cv.notify_all()
 
     def _run(self, req: Request, admitted: float) -> Result:
-        p, uu = req.build()
         try:
+            p, uu = req.build()
             with Domain(p, uu, device=self.device) as d:
                 d.set_precision(req.mixed)
                 dt = req.dt0
@@ -207,18 +216,24 @@ class Server:
             w.join()
 
 
+    def load_bytes(self) -> float:
+        """Current load: footprint bytes of the running jobs plus those of
+        the queued requests, read under the server's lock."""
+        with self._cv:
+            return self._reserved + sum(footprint_bytes(q.nx, q.ny) for q in self._queue)
+
+
 class Router:
     """Several GPUs of one node: one Server per device, each request placed
-    whole on the device with the fewest bytes placed so far plus reserved
-    now (ties to the lower device).  Jobs never span devices, so no
-    collective is involved; results are gathered on the host."""
+    whole on the device with the least current load (footprint bytes of its
+    running and queued jobs; ties to the lower device).  Jobs never span
+    devices, so no collective is involved; results are gathered on the host."""
 
     def __init__(self, devices, budget_bytes: float = 150e9, slots: int = 8,
                  server_cls=None):
         cls = server_cls or Server
         self.servers = [cls(budget_bytes, slots, d) for d in devices]
         self._lock = threading.Lock()
-        self._placed = [0.0] * len(self.servers)  # footprint bytes placed so far
         self.placement: dict = {}
 
     def start_clock(self):
@@ -229,13 +244,12 @@ class Router:
         return self.servers[0].clock()
 
     def submit(self, req: Request):
-        fp = footprint_bytes(req.nx, req.ny)
         with self._lock:
-            k = min(range(len(self.servers)),
-                    key=lambda i: (self._placed[i] + self.servers[i]._reserved, i))
-            self._placed[k] += fp
+            loads = [s.load_bytes() for s in self.servers]
+            k = min(range(len(self.servers)), key=lambda i: (loads[i], i))
             self.placement[req.rid] = self.servers[k].device
-        self.servers[k].submit(req)
+            # submitted under the router's lock, so the next placement sees it
+            self.servers[k].submit(req)
 
     def drain(self):
         for s in self.servers:
@@ -278,13 +292,25 @@ def run_stream(requests, budget_bytes=150e9, slots=8, device=0, realtime=True, d
 
 
 def summarize(results, wall):
+    """Stream statistics.  `cell_updates_per_s` counts every job the GPU ran;
+    `finite_cell_updates_per_s` counts only the jobs that ended with a finite
+    state (no error), and its latencies are over those jobs alone."""
     lat = np.array([r.latency for r in results])
+    ok = [r for r in results if not r.error]
+    lat_ok = np.array([r.latency for r in ok])
     work = float(sum(r.cells * r.steps for r in results))
+    work_ok = float(sum(r.cells * r.steps for r in ok))
+    nonfinite = sum(1 for r in results if r.error and "non-finite" in r.error)
     return {"jobs": len(results), "failed": sum(1 for r in results if r.error),
+            "nonfinite": nonfinite,
             "p50_latency_s": float(np.percentile(lat, 50)) if len(lat) else None,
             "p99_latency_s": float(np.percentile(lat, 99)) if len(lat) else None,
             "cell_updates": work, "wall_s": wall,
-            "cell_updates_per_s": work / wall if wall > 0 else None}
+            "cell_updates_per_s": work / wall if wall > 0 else None,
+            "finite_jobs": len(ok), "finite_cell_updates": work_ok,
+            "finite_cell_updates_per_s": work_ok / wall if wall > 0 else None,
+            "finite_p50_latency_s": float(np.percentile(lat_ok, 50)) if len(lat_ok) else None,
+            "finite_p99_latency_s": float(np.percentile(lat_ok, 99)) if len(lat_ok) else None}
 
 
 def draw_requests(n, seed=5, rate=20.0, sizes=SERVING_SIZES, inverse_cells=True,

@@ -31,11 +31,31 @@ def available() -> bool:
     return os.path.exists(LIB_PATH) and os.path.exists(BIN_PATH)
 
 
-def build(ref_dir: str = "/root/reference") -> None:
+def ref_dir() -> str:
+    """Where the reference's C sources are: $MHD_REF_DIR, else the default
+    of oracle/Makefile (its `REF_DIR ?=` line, the one place that names it)."""
+    env = os.environ.get("MHD_REF_DIR")
+    if env:
+        return env
+    with open(os.path.join(HERE, "Makefile")) as f:
+        for line in f:
+            m = line.split("?=", 1)
+            if len(m) == 2 and m[0].strip() == "REF_DIR":
+                return m[1].strip()
+    return ""
+
+
+def sources_present() -> bool:
+    d = ref_dir()
+    return bool(d) and os.path.isfile(os.path.join(d, "calcDerivs.c"))
+
+
+def build(src_dir: str | None = None) -> None:
     """Compile the reference from its sources (needs the reference tree)."""
-    if not os.path.isdir(ref_dir):
-        raise FileNotFoundError(ref_dir)
-    subprocess.run(["make", "-s", "-C", HERE, f"REF_DIR={ref_dir}"], check=True)
+    d = src_dir or ref_dir()
+    if not d or not os.path.isdir(d):
+        raise FileNotFoundError(d or "MHD_REF_DIR")
+    subprocess.run(["make", "-s", "-C", HERE, f"REF_DIR={d}"], check=True)
 
 
 def _ptr(a: np.ndarray):

@@ -133,3 +133,48 @@ def test_job_record_fields():
     assert rec["latency_s"] == 3.0 and rec["queued_s"] == 1.0
     assert rec["cell_updates_per_s"] == 128 * 128 * 100 / 2.0
     assert rec["cross_helicity"] == 0.1 and rec["error"] is None
+
+
+class _BrokenRequest(S.Request):
+    def build(self):
+        raise RuntimeError("initial condition could not be built")
+
+
+def test_failed_build_is_the_jobs_error_and_releases_its_bytes():
+    # the real Server._run: the build raises before any device work
+    budget = S.footprint_bytes(256, 256)
+    srv = S.Server(budget, slots=1)
+    srv.start_clock()
+    srv.submit(_BrokenRequest(0, 256, 256, 10))
+    srv.submit(_BrokenRequest(1, 256, 256, 10))   # fits only once the first has released
+    srv.drain()                                   # returns: nothing leaked
+    assert sorted(r.rid for r in srv.results) == [0, 1]
+    assert all("could not be built" in r.error for r in srv.results)
+    assert srv._reserved == 0
+
+
+def test_summary_counts_finite_jobs_apart():
+    res = [S.Result(i, 100, 10, 0.0, 0.0, float(i + 1), 1e-3, 1.0,
+                    None, "non-finite state (NaN or Inf) at the end of the job" if i % 4 == 0 else None)
+           for i in range(100)]
+    s = S.summarize(res, 100.0)
+    assert s["nonfinite"] == 25 and s["finite_jobs"] == 75
+    assert s["cell_updates_per_s"] == 100 * 100 * 10 / 100.0
+    assert s["finite_cell_updates_per_s"] == 75 * 100 * 10 / 100.0
+    ok_lat = [float(i + 1) for i in range(100) if i % 4]
+    assert s["finite_p50_latency_s"] == np.percentile(ok_lat, 50)
+
+
+def test_router_ranks_devices_on_current_load():
+    # device 0 has finished its earlier work: a new request goes there again
+    budget = 4 * S.footprint_bytes(512, 512)
+    r = S.Router([0, 1], budget, slots=1, server_cls=FakeServer)
+    r.start_clock()
+    r.submit(S.Request(0, 512, 512, 100))
+    r.servers[0].drain()                      # device 0 idle again, device 1 never used
+    r.servers[0] = FakeServer(budget, slots=1, device=0)
+    r.servers[0].start_clock()
+    r.submit(S.Request(1, 256, 256, 2000))    # ties: lower device
+    r.submit(S.Request(2, 256, 256, 2000))    # device 0 now busy: goes to 1
+    assert r.placement == {0: 0, 1: 0, 2: 1}
+    r.drain()

@@ -11,6 +11,7 @@ collected last, and runs the same alone or after the other tests.
 """
 import ctypes
 
+import mhd_oracle as O
 import numpy as np
 import pytest
 
@@ -51,6 +52,12 @@ def test_noalloc_dt_matches_context_entry_on_two_calls(cleaning):
             d.synchronize()
             got = out.cpu().numpy()
             assert got[0] == pytest.approx(want_dt, rel=1e-14)
+            # and directly against the oracle's calcDt (timeAdvance.c:38-153)
+            odt, och, ocp = O.calcDt(p, state, dt0)
+            assert got[0] == pytest.approx(odt, rel=1e-14)
+            if cleaning == 2:
+                assert got[1] == pytest.approx(och, rel=1e-14)
+                assert got[2] == pytest.approx(ocp, rel=1e-14)
             if cleaning == 2:
                 assert got[1] == pytest.approx(want_ch, rel=1e-14)
                 assert got[2] == pytest.approx(want_cp, rel=1e-14)
@@ -65,3 +72,28 @@ def test_noalloc_rejects_grids_beyond_its_scratch():
     cp = CParams.from_params(p)
     # rejected on the host before any launch; the pointers are never touched
     assert f(ctypes.c_void_p(16), ctypes.byref(cp), 0.0, ctypes.c_void_p(16), None) == 1
+
+
+def test_noalloc_dt_with_a_nan_cell_matches_context_entry():
+    """A NaN cell (not the first) does not make either entry's step NaN; both
+    agree, and equal the oracle's minimum over the other cells."""
+    import torch
+
+    f = _entry()
+    p, uu = ic.orszag_tang(64, 64, di=0.05)
+    uu = uu.copy()
+    uu[1, 17, 23] = np.nan
+    cp = CParams.from_params(p)
+    with Domain(p) as d:
+        d.set("uu", uu)
+        want = d.calcDt(0.0)
+        out = torch.full((3,), -1.0, dtype=torch.float64, device="cuda:0")
+        assert f(d.device_ptr("uu"), ctypes.byref(cp), 0.0, out.data_ptr(), d.stream_handle()) == 0
+        d.synchronize()
+        got = float(out[0].item())
+    assert np.isfinite(got) and got == pytest.approx(want, rel=1e-14)
+    # the oracle's per-cell steps with the NaN cell left out of the minimum
+    cx, cy = O.cell_speeds(p, uu)
+    dtx = np.minimum(np.minimum(p.dx / cx, p.dx * p.dx / p.resistivity), p.dx * p.dx / p.viscosity)
+    dty = np.minimum(np.minimum(p.dy / cy, p.dy * p.dy / p.resistivity), p.dy * p.dy / p.viscosity)
+    assert got == pytest.approx(float(np.nanmin(np.minimum(dtx, dty))) * p.cfl, rel=1e-14)
