@@ -140,10 +140,15 @@ int mhdgpu_set_precision(mhdgpu_ctx *ctx, int precision);
 int mhdgpu_autotune(mhdgpu_ctx *ctx, int *columns_out);
 
 /* --- diagnostics -------------------------------------------------------- */
-/* total energy, cross helicity (sums times dx*dy) and max|divB| of the last
- * computed derivatives; *finite = 0 if the state holds NaN/Inf or rho,p<=0 */
+/* total energy and cross helicity of the state (sums times dx*dy);
+ * *finite = 0 if the state holds a NaN or an Inf.  (No counterpart in the
+ * reference, which prints energies from its driver, mhd.c:292-299.) */
 int mhdgpu_diagnostics(mhdgpu_ctx *ctx, double *energy, double *cross_helicity,
                        int *finite);
+/* cells of the state holding a NaN or Inf, and finite cells whose density or
+ * pressure is not positive (the reference carries on through such states:
+ * its calcDt only drops their NaN speeds).  No counterpart in the reference. */
+int mhdgpu_state_cells(mhdgpu_ctx *ctx, long *nonfinite, long *nonpositive);
 
 /* --- allocation-free time step ---------------------------------------------
  * No counterpart in the reference.  The CFL time step of calcDt for callers
@@ -153,14 +158,14 @@ int mhdgpu_diagnostics(mhdgpu_ctx *ctx, double *energy, double *cross_helicity,
  * [NVAR][nx][ny] on the current device; d_out: 3 device doubles receiving
  * dt (after the 2% hysteresis against dt0), Ch and Cp (hyperbolic cleaning,
  * else 0); stream: a cudaStream_t (NULL: the default stream), the call is
- * asynchronous on it.  Scratch is a fixed 128 KiB device array held by every
+ * asynchronous on it.  Scratch is a fixed 96 KiB device array held by every
  * GPU that loads the library: nx*ny is limited to 33,554,432 cells, larger
  * grids return MHDGPU_ERR_INVALID.  Calls share that array: calls that
  * overlap on the GPU race and must be serialised by the caller.  The first
  * call on a device looks the array up with that device current; make it
- * before any stream capture begins.  A NaN in the state does not make the
- * result NaN (fmin and fmax drop NaN operands), as in mhdgpu_calc_dt; the
- * reference's loop returns NaN only when its very first cell is NaN.  Use
+ * before any stream capture begins.  States with NaN or non-positive
+ * density give what the reference's calcDt gives (as mhdgpu_calc_dt does):
+ * its MAX/MIN macros per cell and its running minimum over the cells.  Use
  * mhdgpu_diagnostics to detect a non-finite state. */
 int mhdgpu_calc_dt_noalloc(const double *d_uu, const mhdgpu_params *p, double dt0,
                            double *d_out, void *stream);

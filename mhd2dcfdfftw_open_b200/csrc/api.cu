@@ -613,7 +613,17 @@ extern "C" int mhdgpu_diagnostics(mhdgpu_ctx *h, double *energy, double *cross_h
 {
     CTX_OR_FAIL(h);
     if (settle(c)) return mhdgpu_last_error();
-    return mhd::launch_diagnostics(c, energy, cross_helicity, finite);
+    long bad = 0;
+    TRY(mhd::launch_diagnostics(c, energy, cross_helicity, &bad, nullptr));
+    if (finite) *finite = bad == 0;
+    return MHDGPU_OK;
+}
+
+extern "C" int mhdgpu_state_cells(mhdgpu_ctx *h, long *nonfinite, long *nonpositive)
+{
+    CTX_OR_FAIL(h);
+    if (settle(c)) return mhdgpu_last_error();
+    return mhd::launch_diagnostics(c, nullptr, nullptr, nonfinite, nonpositive);
 }
 
 // ---------------------------------------------------------------------------

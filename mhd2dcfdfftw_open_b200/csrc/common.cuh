@@ -139,7 +139,7 @@ int launch_rk(Ctx *c, int iRK);
 int launch_calc_dt(Ctx *c, double dt0, double *dt_out);
 int launch_calc_dt_dev(Ctx *c, int keep_dt);
 int launch_max_divb(Ctx *c, double *out);
-int launch_diagnostics(Ctx *c, double *energy, double *ch, int *finite);
+int launch_diagnostics(Ctx *c, double *energy, double *ch, long *nonfinite, long *nonpositive);
 int xline_setup(Ctx *c);
 void xline_free(Ctx *c);
 int fused_setup(Ctx *c);

@@ -115,50 +115,77 @@ __device__ __forceinline__ double warp_sum(double v)
     return v;
 }
 
+// per block: the (mn, lastneg, nanflag) fold of dtcore.cuh at part[3 b ..]
 __global__ void dt_partial_kernel(DtArgs a)
 {
-    double mn = INFINITY;
+    DtFold f{INFINITY, -1.0, 0.0};
     for (long o = blockIdx.x * (long)blockDim.x + threadIdx.x; o < a.plane;
-         o += (long)gridDim.x * blockDim.x) {
-        mn = fmin(mn, cell_dt(a, o));
+         o += (long)gridDim.x * blockDim.x)
+        dt_cell_fold(a, o, f);
+    __shared__ double sm[3][PT / 32];
+    f.mn = warp_min(f.mn);
+    f.lastneg = warp_max(f.lastneg);
+    f.nanflag = warp_max(f.nanflag);
+    if ((threadIdx.x & 31) == 0) {
+        sm[0][threadIdx.x >> 5] = f.mn;
+        sm[1][threadIdx.x >> 5] = f.lastneg;
+        sm[2][threadIdx.x >> 5] = f.nanflag;
     }
-    __shared__ double sm[PT / 32];
-    mn = warp_min(mn);
-    if ((threadIdx.x & 31) == 0) sm[threadIdx.x >> 5] = mn;
     __syncthreads();
-    if (threadIdx.x < 32) {
-        double v = threadIdx.x < blockDim.x / 32 ? sm[threadIdx.x] : INFINITY;
-        v = warp_min(v);
-        if (threadIdx.x == 0) a.part[blockIdx.x] = v;
+    if (threadIdx.x == 0) {
+        double m = INFINITY, l = -1.0, n = 0.0;
+        for (int w = 0; w < (int)(blockDim.x / 32); w++) {
+            m = fmin(m, sm[0][w]);
+            l = fmax(l, sm[1][w]);
+            n = fmax(n, sm[2][w]);
+        }
+        a.part[3 * blockIdx.x] = m;
+        a.part[3 * blockIdx.x + 1] = l;
+        a.part[3 * blockIdx.x + 2] = n;
     }
 }
 
-// scal[0] = dt after the 2% hysteresis (timeAdvance.c:142-152); with
-// hyperbolic cleaning scal[1] = Ch = max(cmaxx, cmaxy) of the LAST cell of
-// the reference's loop (timeAdvance.c:107-112) and scal[2] = Cp = sqrt(Cr Ch)
+// scal[0] = the new dt: the reference's running minimum (dtcore.cuh) times
+// cfl, with the 2% hysteresis of timeAdvance.c:144-151 around dt0 (dt0 is
+// scal[0] itself with dev_dt; keep_dt leaves scal[0] alone); with hyperbolic
+// cleaning scal[1] = Ch = MAX(cmaxx, cmaxy) of the LAST cell of the
+// reference's loop (timeAdvance.c:107-112) and scal[2] = Cp = sqrt(Cr Ch)
 // (divBcleaning.c:4-10).
-// scal[0] = the new dt (hysteresis of timeAdvance.c:144-151 around dt0;
-// dt0 is scal[0] itself with dev_dt, and scal[0] is left alone with keep_dt),
-// scal[1..2] = Ch, Cp of hyperbolic cleaning
-__global__ void dt_final_kernel(DtArgs a, int nparts, double cfl, double dt0, int cleaning,
+__global__ void __launch_bounds__(256) dt_final_kernel(DtArgs a, int nparts, double cfl, double dt0, int cleaning,
                                 double *scal, int dev_dt, int keep_dt)
 {
-    double mn = INFINITY;
-    for (int i = threadIdx.x; i < nparts; i += blockDim.x) mn = fmin(mn, a.part[i]);
-    __shared__ double sm[32];
+    double mn = INFINITY, l = -1.0, n = 0.0;
+    for (int i = threadIdx.x; i < nparts; i += blockDim.x) {
+        mn = fmin(mn, a.part[3 * i]);
+        l = fmax(l, a.part[3 * i + 1]);
+        n = fmax(n, a.part[3 * i + 2]);
+    }
+    __shared__ double sm[3][32];
     mn = warp_min(mn);
-    if ((threadIdx.x & 31) == 0) sm[threadIdx.x >> 5] = mn;
+    l = warp_max(l);
+    n = warp_max(n);
+    if ((threadIdx.x & 31) == 0) {
+        sm[0][threadIdx.x >> 5] = mn;
+        sm[1][threadIdx.x >> 5] = l;
+        sm[2][threadIdx.x >> 5] = n;
+    }
     __syncthreads();
+    mn = INFINITY, l = -1.0, n = 0.0;
+    for (int w = 0; w < (int)(blockDim.x / 32); w++) {
+        mn = fmin(mn, sm[0][w]);
+        l = fmax(l, sm[1][w]);
+        n = fmax(n, sm[2][w]);
+    }
+    __shared__ double red[32];
+    const double dmin = dt_resolve(a, mn, l, n, red);  // uniform across the block
     if (threadIdx.x == 0) {
-        double v = INFINITY;
-        for (int w = 0; w < (int)(blockDim.x / 32); w++) v = fmin(v, sm[w]);
-        double dtmin = v * cfl;
+        double dtmin = dmin * cfl;
         if (dev_dt) dt0 = scal[0];
         if (!keep_dt) scal[0] = (dt0 < 0.98 * dtmin || dt0 > 1.02 * dtmin) ? dtmin : dt0;
         if (cleaning == 2) {
             double cx, cy;
             cell_speeds(a, a.plane - 1, cx, cy);
-            double ch = fmax(cx, cy);
+            double ch = ref_max(cx, cy);
             scal[1] = ch;
             scal[2] = sqrt(0.18 * ch);
         }
@@ -188,7 +215,7 @@ __global__ void maxdivb_kernel(const double *__restrict__ dudx, const double *__
 
 __global__ void diag_kernel(const double *__restrict__ uu, long plane, double gamma, double *part)
 {
-    double e = 0.0, h = 0.0, bad = 0.0;
+    double e = 0.0, h = 0.0, bad = 0.0, neg = 0.0;
     for (long o = blockIdx.x * (long)blockDim.x + threadIdx.x; o < plane;
          o += (long)gridDim.x * blockDim.x) {
         double rho = uu[RHO * plane + o], ux = uu[UX * plane + o], uy = uu[UY * plane + o];
@@ -198,18 +225,23 @@ __global__ void diag_kernel(const double *__restrict__ uu, long plane, double ga
              p / (gamma - 1.0);
         h += ux * bx + uy * by + uz * bz;
         double s = rho + ux + uy + uz + bx + by + bz + p;
-        if (!isfinite(s) || !(rho > 0) || !(p > 0)) bad += 1.0;
+        if (!isfinite(s)) bad += 1.0;                          // a NaN or Inf in the cell
+        else if (!(rho > 0) || !(p > 0)) neg += 1.0;           // finite, rho or p not positive
     }
-    __shared__ double sm[3][PT / 32];
-    e = warp_sum(e); h = warp_sum(h); bad = warp_sum(bad);
+    __shared__ double sm[4][PT / 32];
+    e = warp_sum(e); h = warp_sum(h); bad = warp_sum(bad); neg = warp_sum(neg);
     if ((threadIdx.x & 31) == 0) {
-        sm[0][threadIdx.x >> 5] = e; sm[1][threadIdx.x >> 5] = h; sm[2][threadIdx.x >> 5] = bad;
+        sm[0][threadIdx.x >> 5] = e; sm[1][threadIdx.x >> 5] = h;
+        sm[2][threadIdx.x >> 5] = bad; sm[3][threadIdx.x >> 5] = neg;
     }
     __syncthreads();
     if (threadIdx.x == 0) {
-        double s0 = 0, s1 = 0, s2 = 0;
-        for (int w = 0; w < (int)(blockDim.x / 32); w++) { s0 += sm[0][w]; s1 += sm[1][w]; s2 += sm[2][w]; }
-        part[3 * blockIdx.x] = s0; part[3 * blockIdx.x + 1] = s1; part[3 * blockIdx.x + 2] = s2;
+        double s0 = 0, s1 = 0, s2 = 0, s3 = 0;
+        for (int w = 0; w < (int)(blockDim.x / 32); w++) {
+            s0 += sm[0][w]; s1 += sm[1][w]; s2 += sm[2][w]; s3 += sm[3][w];
+        }
+        part[4 * blockIdx.x] = s0; part[4 * blockIdx.x + 1] = s1;
+        part[4 * blockIdx.x + 2] = s2; part[4 * blockIdx.x + 3] = s3;
     }
 }
 
@@ -332,13 +364,13 @@ int launch_calc_dt_dev(Ctx *c, int keep_dt)
 {
     DtArgs a = dt_args(c);
     int g = grid_for(c, a.plane);
-    if (g > c->nred) g = c->nred;
+    if (3 * g > c->nred) g = c->nred / 3;
     prof_begin(c, KC_REDUCE, 7.0 * a.plane * 8.0);
     dt_partial_kernel<<<g, PT, 0, c->stream>>>(a);
     prof_end(c);
     MHD_CHECK_LAUNCH();
     prof_begin(c, KC_REDUCE, 0.0);
-    dt_final_kernel<<<1, 1024, 0, c->stream>>>(a, g, c->p.cfl, 0.0, c->p.divBcleaning, c->dscal, 1,
+    dt_final_kernel<<<1, 256, 0, c->stream>>>(a, g, c->p.cfl, 0.0, c->p.divBcleaning, c->dscal, 1,
                                                keep_dt);
     prof_end(c);
     MHD_CHECK_LAUNCH();
@@ -349,13 +381,13 @@ int launch_calc_dt(Ctx *c, double dt0, double *dt_out)
 {
     DtArgs a = dt_args(c);
     int g = grid_for(c, a.plane);
-    if (g > c->nred) g = c->nred;
+    if (3 * g > c->nred) g = c->nred / 3;
     prof_begin(c, KC_REDUCE, 7.0 * a.plane * 8.0);
     dt_partial_kernel<<<g, PT, 0, c->stream>>>(a);
     prof_end(c);
     MHD_CHECK_LAUNCH();
     prof_begin(c, KC_REDUCE, 0.0);
-    dt_final_kernel<<<1, 1024, 0, c->stream>>>(a, g, c->p.cfl, dt0, c->p.divBcleaning, c->dscal, 0, 0);
+    dt_final_kernel<<<1, 256, 0, c->stream>>>(a, g, c->p.cfl, dt0, c->p.divBcleaning, c->dscal, 0, 0);
     prof_end(c);
     MHD_CHECK_LAUNCH();
     double h[3];
@@ -389,25 +421,26 @@ int launch_max_divb(Ctx *c, double *out)
     return MHDGPU_OK;
 }
 
-int launch_diagnostics(Ctx *c, double *energy, double *ch, int *finite)
+int launch_diagnostics(Ctx *c, double *energy, double *ch, long *nonfinite, long *nonpositive)
 {
     long plane = c->nx * c->ny;
     int g = grid_for(c, plane);
-    if (3 * g > c->nred) g = c->nred / 3;
+    if (4 * g > c->nred) g = c->nred / 4;
     prof_begin(c, KC_REDUCE, 8.0 * plane * 8.0);
     diag_kernel<<<g, PT, 0, c->stream>>>(c->arr[MHDGPU_UU], plane, c->p.adiabaticIdx, c->dred);
     prof_end(c);
     MHD_CHECK_LAUNCH();
     prof_begin(c, KC_REDUCE, 0.0);
-    reduce_final_kernel<<<1, 32, 0, c->stream>>>(c->dred, g, 3, 1, c->dscal + 4);
+    reduce_final_kernel<<<1, 32, 0, c->stream>>>(c->dred, g, 4, 1, c->dscal + 4);
     prof_end(c);
     MHD_CHECK_LAUNCH();
-    double h[3];
+    double h[4];
     MHD_CUDA_TRY(cudaMemcpyAsync(h, c->dscal + 4, sizeof h, cudaMemcpyDeviceToHost, c->stream));
     MHD_CUDA_TRY(cudaStreamSynchronize(c->stream));
     if (energy) *energy = h[0] * c->dx * c->dy;
     if (ch) *ch = h[1] * c->dx * c->dy;
-    if (finite) *finite = h[2] == 0.0;
+    if (nonfinite) *nonfinite = (long)h[2];
+    if (nonpositive) *nonpositive = (long)h[3];
     return MHDGPU_OK;
 }
 

@@ -4,7 +4,9 @@
 //      two real fields packed as one complex row, one forward FFT, then per
 //      operator a symbol multiply and one inverse FFT -- d/dy of all fields,
 //      d2/dy2 of u and B, d/dy of Ex and Ez (E = -u x B, calcRHS.c:24-43,
-//      formed while the row is loaded);
+//      formed while the row is loaded).  Pairs never mix the out-of-plane
+//      family (uz, Bz, Ex, Ey) with an in-plane field, so fields that the
+//      reference's per-field real transforms keep exactly zero stay zero;
 //   2. calcRHS (calcRHS.c:46-75, 498-544) and rkExecute (timeAdvance.c:29-36)
 //      point by point;
 //   3. the spectral y filter (filteringY, filtering.c:40-94) of the updated
@@ -241,24 +243,39 @@ __global__ void __launch_bounds__(YR_THREADS, (YRGeom<L, T>::MINB)) yrow_kernel(
             yr_op<L, T, false>(tw, A, j, valid, s1, f(a.dudy, fa), fb >= 0 ? f(a.dudy, fb) : nullptr);
         }
     }
-    if (a.mode != 2) {  // (Ex, Ez) = (uz By - uy Bz, uy Bx - ux By), formed in FP64
-        auto efield = [&](size_t o, double &ex, double &ez) {
+    if (a.mode != 2) {
+        // E = -u x B formed in FP64; d/dy of Ex and Ez.  Ex is transformed
+        // with Ey (whose d/dy is not needed) and Ez alone, so that the
+        // out-of-plane family (uz, Bz, Ex, Ey) never shares a transform with
+        // an in-plane field: a field the reference keeps exactly zero (2-D
+        // flows) stays exactly zero here too, instead of picking up the
+        // rounding of its partner in the packed complex transform.
+        auto efield = [&](size_t o, double &ex, double &ey, double &ez) {
             const double *u = a.uu + o;
             double ux = u[UX * plane], uy = u[UY * plane], uz = u[UZ * plane];
             double bx = u[BX * plane], by = u[BY * plane], bz = u[BZ * plane];
             ex = uz * by - uy * bz;
+            ey = ux * bz - uz * bx;
             ez = uy * bx - ux * by;
         };
-        double cx = 0.0, cz = 0.0;
-        if (MIX && valid) efield(ro, cx, cz);
+        double cx = 0.0, cy = 0.0, cz = 0.0;
+        if (MIX && valid) efield(ro, cx, cy, cz);
 #pragma unroll 4
         for (int m = 0; m < 16; m++) {
             const int i = j + m * G::T_;
-            double ex = 0.0, ez = 0.0;
-            if (valid) efield(ro + i, ex, ez);
-            A[fpad(i)] = cmk<C>((T)(ex - cx), (T)(ez - cz));
+            double ex = 0.0, ey = 0.0, ez = 0.0;
+            if (valid) efield(ro + i, ex, ey, ez);
+            A[fpad(i)] = cmk<C>((T)(ex - cx), (T)(ey - cy));
         }
-        yr_op<L, T, false>(tw, A, j, valid, s1, f(a.dEdy, 0), f(a.dEdy, 2));
+        yr_op<L, T, false>(tw, A, j, valid, s1, f(a.dEdy, 0), (T *)nullptr);
+#pragma unroll 4
+        for (int m = 0; m < 16; m++) {
+            const int i = j + m * G::T_;
+            double ex = 0.0, ey = 0.0, ez = 0.0;
+            if (valid) efield(ro + i, ex, ey, ez);
+            A[fpad(i)] = cmk<C>((T)(ez - cz), (T)0);
+        }
+        yr_op<L, T, false>(tw, A, j, valid, s1, f(a.dEdy, 2), (T *)nullptr);
     }
 
     if (a.mode == 1) return;  // uniform across the grid
@@ -331,9 +348,11 @@ __global__ void __launch_bounds__(YR_THREADS, (YRGeom<L, T>::MINB)) yrow_kernel(
     // FP64: the filtered row replaces the row.  FP32: the filter minus the
     // identity is applied to the shifted row and its result added to the
     // FP64 row.
-    const int nfp = (a.nvar + 1) / 2;
+    // the pairs of the derivatives: (ux, uy) (rho, p) (uz, Bz) (Bx, By) [psi]
+    const int nfp = a.nvar == 9 ? 5 : 4;
     for (int q = 0; q < nfp; q++) {
-        const int v = 2 * q, w = v + 1 < a.nvar ? v + 1 : -1;
+        const int v = q == 0 ? UX : q == 1 ? RHO : q == 2 ? UZ : q == 3 ? BX : PSI;
+        const int w = q == 0 ? UY : q == 1 ? P : q == 2 ? BZ : q == 3 ? BY : -1;
         double *ra = su(v), *rb = w >= 0 ? su(w) : nullptr;
         const double ca = sh(ra), cb = rb ? sh(rb) : 0.0;
         yr_load<L, T>(A, ra, rb, ca, cb, j, valid);

@@ -4,7 +4,8 @@
 // r2c -> multiply -> c2r round trip per (field, x-row).
 //
 // B200 design.  y is contiguous, so a CTA owns whole rows.  Two real rows a, b
-// are packed as one complex row z = a + i b and transformed by a complex FFT
+// (paired as launch_yspec says) are packed as one complex row z = a + i b and
+// transformed by a complex FFT
 // of length ny held in shared memory (radix-4 Stockham passes, one radix-2
 // pass when log2 ny is odd).  Every operator here is real (its symbol s obeys
 // s(-k) = conj s(k)), so multiplying Z[k] by s over the full signed spectrum
@@ -113,16 +114,18 @@ struct YArgs {
     int logN;
     int nv;
     int in_start, out_start;
+    int pa[5], pb[5];  // the fields of each pair (pb < 0: none)
 };
 
 // One (x-row, field pair) per CTA: out[v] = op(in[in_start + v]) for the two
-// fields v = 2*pair, 2*pair+1 of row blockIdx.x.
+// fields v = pa[pair], pb[pair] of row blockIdx.x.
 __global__ void __launch_bounds__(YT) yspec_kernel(YArgs a)
 {
     extern __shared__ __align__(16) double2 zsm[];
     const int N = (int)a.ny;
     const long row = blockIdx.x;
-    const int v0 = 2 * blockIdx.y, v1 = v0 + 1;
+    const int v0 = a.pa[blockIdx.y];
+    const int v1 = a.pb[blockIdx.y] >= 0 ? a.pb[blockIdx.y] : a.nv;  // nv: none
     const size_t plane = (size_t)a.nx * a.ny;
     const double *ra = a.in + (size_t)(a.in_start + v0) * plane + row * a.ny;
     const double *rb = v1 < a.nv ? a.in + (size_t)(a.in_start + v1) * plane + row * a.ny : nullptr;
@@ -230,7 +233,28 @@ int launch_yspec(Ctx *c, int op, int nv, const double *in, int in_start, double 
     a.nv = nv;
     a.in_start = in_start;
     a.out_start = out_start;
-    dim3 grid((unsigned)c->nx, (unsigned)((nv + 1) / 2), 1);
+    // Which fields share a complex transform.  A whole state (8 or 9 fields
+    // from field 0) is paired (ux, uy) (rho, p) (uz, Bz) (Bx, By) [psi], so
+    // that the out-of-plane family never shares a transform with an in-plane
+    // field and a field the reference keeps exactly zero (uz, Bz of a 2-D
+    // flow) stays exactly zero; 3-field sets (u, B, E) pair (x, y) and leave
+    // z alone; other sets pair consecutive fields.
+    int np = 0;
+    if (nv >= 8 && nv <= 9 && in_start == 0 && out_start == 0) {
+        const int pa[5] = {UX, RHO, UZ, BX, PSI}, pb[5] = {UY, P, BZ, BY, -1};
+        np = nv == 9 ? 5 : 4;
+        for (int q = 0; q < np; q++) {
+            a.pa[q] = pa[q];
+            a.pb[q] = pb[q];
+        }
+    } else {
+        if (nv > 10) return mhd_set_error(MHDGPU_ERR_INVALID);
+        for (int v = 0; v < nv; v += 2, np++) {
+            a.pa[np] = v;
+            a.pb[np] = v + 1 < nv ? v + 1 : -1;
+        }
+    }
+    dim3 grid((unsigned)c->nx, (unsigned)np, 1);
     int thr = (int)std::min<long>(YT, std::max<long>(32, c->ny / 4));
     prof_begin(c, KC_YSPEC, (double)c->nx * c->ny * 8.0 * 2.0 * nv);
     yspec_kernel<<<grid, thr, sizeof(double2) * c->ny, c->stream>>>(a);

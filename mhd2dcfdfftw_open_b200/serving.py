@@ -90,6 +90,7 @@ class Result:
     uu: np.ndarray | None = None
     error: str | None = None
     cross_helicity: float = float("nan")
+    positive: bool = True     # every cell's density and pressure > 0 at the end
 
     @property
     def latency(self) -> float:
@@ -103,7 +104,7 @@ class Result:
                 "energy": self.energy, "cross_helicity": self.cross_helicity,
                 "latency_s": self.latency, "queued_s": self.admitted - self.arrival,
                 "cell_updates_per_s": self.cells * self.steps / busy if busy > 0 else None,
-                "error": self.error}
+                "positive": self.positive, "error": self.error}
 
 
 class Server:
@@ -188,10 +189,13 @@ class Server:
                     left -= n
                 diag = d.diagnostics()
                 out = d.get("uu") if req.keep_state else None
-            # a state that left the finite numbers is this job's error, not the server's
+            # a state that left the finite numbers is this job's error, not the
+            # server's; a finite state with a non-positive density or pressure
+            # (which the reference also carries on with) is flagged, not failed
             err = None if diag["finite"] else "non-finite state (NaN or Inf) at the end of the job"
             return Result(req.rid, req.nx * req.ny, req.steps, req.arrival, admitted,
-                          self.clock(), dt, diag["energy"], out, err, diag["cross_helicity"])
+                          self.clock(), dt, diag["energy"], out, err, diag["cross_helicity"],
+                          diag["positive"])
         except Exception as exc:  # reported per job, the server keeps serving
             return Result(req.rid, req.nx * req.ny, req.steps, req.arrival, admitted,
                           self.clock(), 0.0, float("nan"), None, str(exc))
@@ -301,8 +305,9 @@ def summarize(results, wall):
     work = float(sum(r.cells * r.steps for r in results))
     work_ok = float(sum(r.cells * r.steps for r in ok))
     nonfinite = sum(1 for r in results if r.error and "non-finite" in r.error)
+    nonpositive = sum(1 for r in results if not r.error and not r.positive)
     return {"jobs": len(results), "failed": sum(1 for r in results if r.error),
-            "nonfinite": nonfinite,
+            "nonfinite": nonfinite, "finite_but_nonpositive": nonpositive,
             "p50_latency_s": float(np.percentile(lat, 50)) if len(lat) else None,
             "p99_latency_s": float(np.percentile(lat, 99)) if len(lat) else None,
             "cell_updates": work, "wall_s": wall,

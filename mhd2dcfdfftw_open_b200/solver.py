@@ -42,7 +42,7 @@ EXPORTED = (
     "mhdgpu_calc_efield", "mhdgpu_calc_divb", "mhdgpu_calc_rhs", "mhdgpu_rk_init",
     "mhdgpu_rk_execute", "mhdgpu_filtering", "mhdgpu_calc_dt", "mhdgpu_check_divb",
     "mhdgpu_get_cleaning_speeds", "mhdgpu_stage", "mhdgpu_steps", "mhdgpu_steps_fused",
-    "mhdgpu_diagnostics", "mhdgpu_stream", "mhdgpu_launch_count", "mhdgpu_profile",
+    "mhdgpu_diagnostics", "mhdgpu_state_cells", "mhdgpu_stream", "mhdgpu_launch_count", "mhdgpu_profile",
     "mhdgpu_profile_read", "mhdgpu_set_precision", "mhdgpu_autotune", "mhdgpu_selftest_wait",
 )
 
@@ -98,6 +98,7 @@ def load_library(path: str = LIB_PATH):
     L.mhdgpu_autotune.argtypes = [vp, ctypes.POINTER(ctypes.c_int)]
     L.mhdgpu_selftest_wait.argtypes = [vp, ctypes.c_double]
     L.mhdgpu_diagnostics.argtypes = [vp, dp, dp, ctypes.POINTER(ctypes.c_int)]
+    L.mhdgpu_state_cells.argtypes = [vp, ctypes.POINTER(ctypes.c_long), ctypes.POINTER(ctypes.c_long)]
     L.mhdgpu_stream.argtypes = [vp]
     L.mhdgpu_stream.restype = vp
     L.mhdgpu_launch_count.argtypes = [vp]
@@ -251,7 +252,11 @@ class Domain:
         e, h, fin = ctypes.c_double(), ctypes.c_double(), ctypes.c_int()
         self._check(self.lib.mhdgpu_diagnostics(self.h, ctypes.byref(e), ctypes.byref(h),
                                                 ctypes.byref(fin)))
-        return {"energy": e.value, "cross_helicity": h.value, "finite": bool(fin.value)}
+        nf, npos = ctypes.c_long(), ctypes.c_long()
+        self._check(self.lib.mhdgpu_state_cells(self.h, ctypes.byref(nf), ctypes.byref(npos)))
+        return {"energy": e.value, "cross_helicity": h.value, "finite": bool(fin.value),
+                "nonfinite_cells": nf.value, "nonpositive_cells": npos.value,
+                "positive": nf.value == 0 and npos.value == 0}
 
     @property
     def uu(self):

@@ -308,54 +308,102 @@ def rkExecute(uu, dudt, dudtRK, iRK, dt):
     return uu + c * dudt + d * dudtRK, dudt.copy()
 
 
+def MAX(a, b):
+    """The reference's MAX (macros.h:26): b whenever a > b is false, which
+    includes a NaN on either side."""
+    return np.where(a > b, a, b)
+
+
+def MIN(a, b):
+    """The reference's MIN (macros.h:27)."""
+    return np.where(a < b, a, b)
+
+
 def cell_speeds(p, uu):
-    """Per-cell cmaxx, cmaxy of calcDt (timeAdvance.c:50-105)."""
+    """Per-cell cmaxx, cmaxy of calcDt (timeAdvance.c:50-105), with the
+    reference's MAX/MIN so that NaN cells come out as they do there."""
     g = p.adiabaticIdx
-    rho = uu[RHO]
-    csound2 = g * uu[P] / rho
-    sr = np.sqrt(rho)
-    cax = uu[BX] / sr
-    cay = uu[BY] / sr
-    caz = uu[BZ] / sr
-    ca2 = cax * cax + cay * cay + caz * caz
-    cms2 = csound2 + ca2
-    cnsx2 = np.sqrt(np.maximum(cms2 * cms2 - 4 * csound2 * cax * cax, 0.))
-    cnsy2 = np.sqrt(np.maximum(cms2 * cms2 - 4 * csound2 * cay * cay, 0.))
-    cfx = np.sqrt(cms2 + cnsx2) / np.sqrt(2.)
-    cfy = np.sqrt(cms2 + cnsy2) / np.sqrt(2.)
-    csx = np.sqrt(np.maximum(cms2 - cnsx2, 0.)) / np.sqrt(2.)
-    csy = np.sqrt(np.maximum(cms2 - cnsy2, 0.)) / np.sqrt(2.)
-    ux, uy = uu[UX], uu[UY]
-    cmaxx = np.maximum.reduce([np.abs(ux), np.abs(ux - cax), np.abs(ux - csx), np.abs(ux - cfx),
-                               np.abs(ux + cax), np.abs(ux + csx), np.abs(ux + cfx)])
-    cmaxy = np.maximum.reduce([np.abs(uy), np.abs(uy - cay), np.abs(uy - csy), np.abs(uy - cfy),
-                               np.abs(uy + cay), np.abs(uy + csy), np.abs(uy + cfy)])
-    if p.Hall == 1:
-        ch = p.di / min(p.dx, p.dy) / rho * np.maximum(np.abs(uu[BX]),
-                                                      np.maximum(np.abs(uu[BY]), np.abs(uu[BZ])))
-        cmaxx = np.maximum(cmaxx, ch)
-        cmaxy = np.maximum(cmaxy, ch)
+    with np.errstate(invalid="ignore", divide="ignore"):
+        rho = uu[RHO]
+        csound2 = g * uu[P] / rho
+        sr = np.sqrt(rho)
+        cax = uu[BX] / sr
+        cay = uu[BY] / sr
+        caz = uu[BZ] / sr
+        ca2 = cax * cax + cay * cay + caz * caz
+        cms2 = csound2 + ca2
+        cnsx2 = np.sqrt(MAX(cms2 * cms2 - 4 * csound2 * cax * cax, 0.))
+        cnsy2 = np.sqrt(MAX(cms2 * cms2 - 4 * csound2 * cay * cay, 0.))
+        cfx = np.sqrt(cms2 + cnsx2) / np.sqrt(2.)
+        cfy = np.sqrt(cms2 + cnsy2) / np.sqrt(2.)
+        csx = np.sqrt(MAX(cms2 - cnsx2, 0.)) / np.sqrt(2.)
+        csy = np.sqrt(MAX(cms2 - cnsy2, 0.)) / np.sqrt(2.)
+        ux, uy = uu[UX], uu[UY]
+        cmaxx = MAX(np.abs(ux), np.abs(ux - cax))
+        for t in (np.abs(ux - csx), np.abs(ux - cfx), np.abs(ux + cax), np.abs(ux + csx),
+                  np.abs(ux + cfx)):
+            cmaxx = MAX(t, cmaxx)
+        cmaxy = MAX(np.abs(uy), np.abs(uy - cay))
+        for t in (np.abs(uy - csy), np.abs(uy - cfy), np.abs(uy + cay), np.abs(uy + csy),
+                  np.abs(uy + cfy)):
+            cmaxy = MAX(t, cmaxy)
+        if p.Hall == 1:
+            ch = p.di / min(p.dx, p.dy) / rho * MAX(np.abs(uu[BX]),
+                                                    MAX(np.abs(uu[BY]), np.abs(uu[BZ])))
+            cmaxx = MAX(cmaxx, ch)
+            cmaxy = MAX(cmaxy, ch)
     return cmaxx, cmaxy
+
+
+def cell_dt(p, uu):
+    """MIN(dtx, dty) per cell with the diffusive limits (timeAdvance.c:114-129)."""
+    cmaxx, cmaxy = cell_speeds(p, uu)
+    with np.errstate(invalid="ignore", divide="ignore"):
+        dtx = p.dx / cmaxx
+        dty = p.dy / cmaxy
+        if p.resistivity > 0:
+            dtx = MIN(dtx, p.dx * p.dx / p.resistivity)
+            dty = MIN(dty, p.dy * p.dy / p.resistivity)
+        if p.viscosity > 0:
+            dtx = MIN(dtx, p.dx * p.dx / p.viscosity)
+            dty = MIN(dty, p.dy * p.dy / p.viscosity)
+        return MIN(dtx, dty), cmaxx, cmaxy
+
+
+def running_min(v):
+    """The reference's minimum over the cells in loop order
+    (timeAdvance.c:47, 131-134): dtmin = -1, then per cell
+    `if (dtmin < 0 || v < dtmin) dtmin = v`.  A negative dtmin is replaced by
+    the next cell whatever it is, NaN included (and a NaN dtmin never
+    changes again).  Hence: NaN if a NaN cell comes first or right after a
+    negative cell; else, after the last negative cell, that cell itself if it
+    is the last, or the minimum of the cells after it (NaN cells skipped)."""
+    v = np.asarray(v, dtype=np.float64)
+    nan = np.isnan(v)
+    neg = v < 0
+    after_neg = np.concatenate(([True], neg[:-1]))
+    if np.any(nan & after_neg):
+        return float("nan")
+    if not neg.any():
+        return float(np.nanmin(v)) if not nan.all() else float("nan")
+    last = int(np.flatnonzero(neg)[-1])
+    if last == len(v) - 1:
+        return float(v[last])
+    return float(np.nanmin(v[last + 1:]))
 
 
 def calcDt(p, uu, dt0):
     """calcDt (timeAdvance.c:38-153).  Returns (dt, Ch, Cp); with hyperbolic
     cleaning Ch is max(cmaxx, cmaxy) of the LAST cell of the loop
-    (timeAdvance.c:107-112) and Cp = sqrt(Cr*Ch) (divBcleaning.c:7-10)."""
-    cmaxx, cmaxy = cell_speeds(p, uu)
-    dtx = p.dx / cmaxx
-    dty = p.dy / cmaxy
-    if p.resistivity > 0:
-        dtx = np.minimum(dtx, p.dx * p.dx / p.resistivity)
-        dty = np.minimum(dty, p.dy * p.dy / p.resistivity)
-    if p.viscosity > 0:
-        dtx = np.minimum(dtx, p.dx * p.dx / p.viscosity)
-        dty = np.minimum(dty, p.dy * p.dy / p.viscosity)
-    dtmin = float(np.min(np.minimum(dtx, dty))) * p.cfl
+    (timeAdvance.c:107-112) and Cp = sqrt(Cr*Ch) (divBcleaning.c:7-10).
+    The minimum over the cells is the reference's running minimum
+    (running_min)."""
+    cdt, cmaxx, cmaxy = cell_dt(p, uu)
+    dtmin = running_min(cdt.ravel()) * p.cfl
     dt = dtmin if (dt0 < 0.98 * dtmin or dt0 > 1.02 * dtmin) else dt0
     Ch = Cp = 0.0
     if p.divBcleaning == 2:
-        Ch = float(max(cmaxx[-1, -1], cmaxy[-1, -1]))
+        Ch = float(MAX(cmaxx[-1, -1], cmaxy[-1, -1]))
         Cp = math.sqrt(CR_DIVB_CLEANING * Ch)
     return dt, Ch, Cp
 

@@ -8,8 +8,10 @@
 * A drawn serving job that leaves the finite numbers (Orszag-Tang 128^2,
   d_i = 0.0933, eta = nu = 1.2185e-4, CFL 0.3, request 9 of the seeded
   100-request stream): the FP64 GPU path and the reference advance in
-  lockstep, 10 steps at a time, agree while the state is finite, and turn
-  non-finite at the same 10-step checkpoint.
+  lockstep, 10 steps at a time, agree to 1e-12 through step 300 (past the
+  step where the pressure turns negative, 237, in both) and to 1e-9 through
+  step 350, and turn non-finite (NaN or Inf) within one 10-step checkpoint
+  of each other (step 370 in the reference).
 * The serving form's precision gate: two jobs served together in mixed
   precision, 1000 steps each, against the same jobs in FP64, per-field
   relative L2 against each field's own norm <= 1e-5.
@@ -77,7 +79,7 @@ def test_diverging_job_matches_reference_until_it_blows_up(reference):
                     ref_bad = s
             if gpu_bad is None:
                 gdt = d.steps(10, 0.0, dt=gdt, fused=True)
-                if not d.diagnostics()["finite"]:
+                if not np.isfinite(d.get("uu")).all():
                     gpu_bad = s
             if ref_bad is None and gpu_bad is None:
                 errs.append((s, float(rel_l2_own(d.get("uu"), reference.uu).max()),
@@ -85,12 +87,16 @@ def test_diverging_job_matches_reference_until_it_blows_up(reference):
             if ref_bad is not None and gpu_bad is not None:
                 break
     print("non-finite at step", ref_bad, "(reference),", gpu_bad, "(GPU)")
-    print("max rel L2 / dt difference every 50 steps:",
-          [(s, f"{e:.2e}", f"{t:.1e}") for s, e, t in errs if s % 50 == 0])
+    print("max rel L2 / dt difference:",
+          [(s, f"{e:.2e}", f"{t:.1e}") for s, e, t in errs if s % 50 == 0 or s > 250])
     assert ref_bad is not None and 300 <= ref_bad <= 420
-    assert gpu_bad == ref_bad
-    # agreement while the flow is still smooth
-    assert max(e for s, e, _ in errs if s <= 250) < 1e-9
+    # The pressure turns negative at step 237 in both and both carry on; the
+    # fields agree to ~1e-13 through step 300 and ~1e-11 through 350.  In the
+    # last steps before the blow-up the scheme amplifies any difference by
+    # about 1e4 per 10 steps, so the NaN arrives within one checkpoint.
+    assert max(e for s, e, _ in errs if s <= 300) < 1e-12
+    assert max(e for s, e, _ in errs if s <= 350) < 1e-9
+    assert gpu_bad is not None and abs(gpu_bad - ref_bad) <= 10
 
 
 def _served(reqs, mixed):
@@ -114,3 +120,17 @@ def test_mixed_serving_field_error_after_1000_steps():
         err = rel_l2_own(mixed[rid], fp64[rid])
         print(f"job {rid}: per-field relative L2 (own norm) after 1000 steps", np.array2string(err, precision=2))
         assert err.max() < TOL_MIXED_1000, err
+
+
+@pytest.mark.parametrize("path", ["operators", "fused", "mixed"])
+def test_out_of_plane_fields_of_a_2d_flow_stay_exactly_zero(path):
+    """uz and Bz of the Orszag-Tang vortex are zero and have no source; the
+    reference's per-field real transforms keep them exactly zero, and so
+    must every GPU path (no rounding leaking in from a packed partner)."""
+    p, uu = ic.orszag_tang(64, 64, di=0.05)
+    with Domain(p, uu) as d:
+        if path == "mixed":
+            d.set_precision(True)
+        d.steps(30, 0.0, dt=1e-4, fused=path != "operators")
+        out = d.get("uu")
+    assert not out[3].any() and not out[6].any()

@@ -129,3 +129,27 @@ def test_uniform_state_is_stationary():
     s = O.State(p, uu)
     O.steps(s, 2, 1e-3)
     assert np.abs(s.uu - uu).max() < 1e-13
+
+
+def test_oracle_calc_dt_matches_reference_on_broken_states(reference):
+    """calcDt on states with NaN, negative density or pressure: the reference's
+    MAX/MIN macros and its running minimum (dtmin = -1, replaced whenever it is
+    negative) give results a plain minimum would not; the oracle's restatement
+    follows them bit for bit."""
+    from mhd2dcfdfftw_open_b200 import ic
+    p, uu = ic.orszag_tang(32, 32, di=0.05)
+    reference.setup(p)
+    rng = np.random.default_rng(11)
+    for k in range(30):
+        u = uu.copy()
+        for _ in range(int(rng.integers(1, 6))):
+            i, j = rng.integers(0, 32, 2)
+            u[rng.choice([0, 1, 7]), i, j] = rng.choice([np.nan, -1.0, -0.5, 1e-9])
+        if k % 5 == 0:
+            u[0, 0, 0] = -1.0
+            u[1, 0, 1] = np.nan
+        if k % 7 == 0:
+            u[0, -1, -1] = -1.0
+        r = reference.calc_dt(u, 1e-3)[0]
+        o = O.calcDt(p, u, 1e-3)[0]
+        assert (np.isnan(r) and np.isnan(o)) or r == o, (k, r, o)
