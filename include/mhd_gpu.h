@@ -188,7 +188,8 @@ int mhdgpu_profile(mhdgpu_ctx *ctx, int enable);
 /* total device time, launch count and algorithmic bytes (what the launches
  * must read and write at least) recorded for a kernel class:
  * 0 x-line solver, 1 y spectral, 2 pointwise, 3 reductions,
- * 4 fused x pass, 5 fused y pass */
+ * 4 fused x pass (x derivatives on long lines), 5 fused y pass,
+ * 6 x filter of the fused steps on long lines */
 int mhdgpu_profile_read(mhdgpu_ctx *ctx, int kclass, double *total_ms, long *count,
                         double *bytes);
 

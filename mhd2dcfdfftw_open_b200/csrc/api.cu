@@ -222,11 +222,13 @@ namespace mhd {
 int fused_apply_pending_filter(Ctx *c);
 }
 
-// Apply the x filter that the fused stage leaves pending, so that every
-// public entry point sees the same state as the reference would hold.
+// Apply the x filter that the fused stage leaves pending (and bring a state
+// settled into the x filter's copy back to uu), so that every public entry
+// point sees the same state as the reference would hold.
 static int settle(Ctx *c)
 {
-    return c->fused_pending_filter ? mhd::fused_apply_pending_filter(c) : MHDGPU_OK;
+    return (c->fused_pending_filter || c->state_in_S) ? mhd::fused_apply_pending_filter(c)
+                                                      : MHDGPU_OK;
 }
 
 extern "C" double *mhdgpu_device_array(mhdgpu_ctx *h, int which)
@@ -245,7 +247,10 @@ extern "C" int mhdgpu_set_array(mhdgpu_ctx *h, int which, const double *host)
     MHD_CUDA_TRY(cudaMemcpyAsync(c->arr[which], host, n * sizeof(double), cudaMemcpyHostToDevice,
                                  c->stream));
     MHD_CUDA_TRY(cudaStreamSynchronize(c->stream));
-    if (which == MHDGPU_UU) c->fused_pending_filter = 0;
+    if (which == MHDGPU_UU) {
+        c->fused_pending_filter = 0;
+        c->state_in_S = 0;
+    }
     return MHDGPU_OK;
 }
 
@@ -471,7 +476,7 @@ static int fused_step_dev(Ctx *c, bool need_dt, bool keep_dt)
 {
     for (int k = 0; k < 3; k++) TRY(mhd::fused_stage(c, k, 0, k == 2));
     if (need_dt) {
-        TRY(settle(c));
+        TRY(mhd::fused_settle_dev(c));
         TRY(mhd::launch_calc_dt_dev(c, keep_dt));
     }
     return MHDGPU_OK;
@@ -522,7 +527,7 @@ extern "C" int mhdgpu_steps_fused(mhdgpu_ctx *h, int nsteps, double dt_fixed, do
     const double dt0 = fixed ? dt_fixed : dt;
     MHD_CUDA_TRY(cudaMemcpyAsync(c->dscal, &dt0, sizeof(double), cudaMemcpyHostToDevice, c->stream));
     if (need_dt) {
-        TRY(settle(c));
+        TRY(mhd::fused_settle_dev(c));
         TRY(mhd::launch_calc_dt_dev(c, fixed));
     }
     c->dev_dt = 1;

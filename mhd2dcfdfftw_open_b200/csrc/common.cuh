@@ -46,7 +46,7 @@ struct XTables {
 
 // kernel classes for the event-timing hooks (mhdgpu_profile_read)
 enum KClass { KC_XSOLVE = 0, KC_YSPEC, KC_POINTWISE, KC_REDUCE, KC_FUSED_X, KC_FUSED_Y,
-              KC_NCLASS };
+              KC_FUSED_XF, KC_NCLASS };
 
 struct Ctx {
     mhdgpu_params p;
@@ -103,6 +103,12 @@ struct Ctx {
     double xf_pw[2][2];   // interior sub-chunk products (-m)^S, (-g)^S per matrix
     double xf_alphaF[2];  // filter matrix off-diagonal: interior, edge rows
     CUtensorMap xl_tmap_big, xl_tmap_unit;  // uu as [nvar*nx rows][ny] for the x pass
+    // chunked x pass of long lines (xfir.cu): the x filter writes the filtered
+    // state to xn_state, from which the derivatives and the y pass read it
+    void *xn;                    // host side (parameter blocks, device tables)
+    int xn_on;                   // the fused steps use it
+    double *xn_state;            // nvar planes
+    int state_in_S;              // the current, x-filtered state is in xn_state
 };
 
 }  // namespace mhd
@@ -124,6 +130,8 @@ void prof_end(mhd::Ctx *c);
 
 // kernels launched by api.cu, defined in the other translation units
 namespace mhd {
+const double *state_ptr(const Ctx *c);
+int fused_settle_dev(Ctx *c);
 int xsolve_setup(Ctx *c);
 void xsolve_free(Ctx *c);
 int launch_xsolve(Ctx *c, int op, int nv, const double *in, int in_start,

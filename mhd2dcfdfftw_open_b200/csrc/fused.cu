@@ -19,17 +19,46 @@
 
 #include "common.cuh"
 #include "xcore.cuh"
+#include "xfir.cuh"
 
 namespace mhd {
 
-int fused_setup(Ctx *c) { return xline_setup(c); }
-void fused_free(Ctx *c) { xline_free(c); }
+bool yrow_supported(const Ctx *c);
+int launch_yrow(Ctx *c, int iRK, int last_stage, int mode);
+
+int fused_setup(Ctx *c)
+{
+    int rc = xline_setup(c);
+    if (rc) return rc;
+    return yrow_supported(c) ? xn_setup(c) : MHDGPU_OK;
+}
+
+void fused_free(Ctx *c)
+{
+    xline_free(c);
+    xn_free(c);
+}
 
 static double planeb(const Ctx *c) { return (double)c->nx * c->ny * 8.0; }
 
-// x pass of a stage: one launch for all fields and the electric field
+// Where the current state is: the x-filtered copy the chunked x filter
+// wrote, or the context's uu.
+const double *state_ptr(const Ctx *c) { return c->state_in_S ? c->xn_state : c->arr[MHDGPU_UU]; }
+
+// x pass of a stage: one launch for all fields and the electric field, or,
+// on long lines, the chunked x filter into the state copy and the chunked
+// derivatives of that copy (xfir.cu)
 static int fused_x_pass(Ctx *c)
 {
+    if (c->xn_on) {
+        if (c->fused_pending_filter) {
+            int rc = launch_xf(c, c->arr[MHDGPU_UU], c->xn_state);
+            if (rc) return rc;
+            c->fused_pending_filter = 0;
+            c->state_in_S = 1;
+        }
+        return launch_xd(c, state_ptr(c));
+    }
     const mhdgpu_params &p = c->p;
     XFArgs a;
     std::memset(&a, 0, sizeof a);
@@ -81,8 +110,37 @@ int fused_x_timing_pass(Ctx *c)
     return rc;
 }
 
+int fused_apply_pending_filter(Ctx *c);
+
+// The pending x filter applied where the next device step reads the state
+// (calcDt, the first stage): with the chunked x pass into the state copy,
+// else in place.
+int fused_settle_dev(Ctx *c)
+{
+    if (!c->xn_on) return fused_apply_pending_filter(c);
+    if (!c->fused_pending_filter) return MHDGPU_OK;
+    int rc = launch_xf(c, c->arr[MHDGPU_UU], c->xn_state);
+    if (rc) return rc;
+    c->fused_pending_filter = 0;
+    c->state_in_S = 1;
+    return MHDGPU_OK;
+}
+
+// The state filtered and in uu, as every entry point outside the fused steps
+// expects it.
 int fused_apply_pending_filter(Ctx *c)
 {
+    if (c->xn_on) {
+        int rc = fused_settle_dev(c);
+        if (rc) return rc;
+        if (c->state_in_S) {
+            MHD_CUDA_TRY(cudaMemcpyAsync(c->arr[MHDGPU_UU], c->xn_state,
+                                         sizeof(double) * c->nvar * c->nx * c->ny,
+                                         cudaMemcpyDeviceToDevice, c->stream));
+            c->state_in_S = 0;
+        }
+        return MHDGPU_OK;
+    }
     if (!c->fused_pending_filter) return MHDGPU_OK;
     XFArgs a;
     std::memset(&a, 0, sizeof a);
@@ -95,9 +153,6 @@ int fused_apply_pending_filter(Ctx *c)
     c->fused_pending_filter = 0;
     return MHDGPU_OK;
 }
-
-bool yrow_supported(const Ctx *c);
-int launch_yrow(Ctx *c, int iRK, int last_stage, int mode);
 
 int fused_stage(Ctx *c, int iRK, int first, int last)
 {
@@ -119,6 +174,7 @@ int fused_stage(Ctx *c, int iRK, int first, int last)
     }
     if (rc) return rc;
     c->fused_pending_filter = 1;
+    c->state_in_S = 0;  // the y pass wrote the new state to uu
     return MHDGPU_OK;
 }
 

@@ -363,6 +363,7 @@ static DtArgs dt_args(Ctx *c)
 int launch_calc_dt_dev(Ctx *c, int keep_dt)
 {
     DtArgs a = dt_args(c);
+    a.uu = state_ptr(c);  // the settled state: in the x filter's copy on long lines
     int g = grid_for(c, a.plane);
     if (3 * g > c->nred) g = c->nred / 3;
     prof_begin(c, KC_REDUCE, 7.0 * a.plane * 8.0);

@@ -28,7 +28,8 @@ namespace mhd {
 constexpr int YR_THREADS = 256;
 
 struct YRArgs {
-    double *uu, *dudtRK;
+    const double *uin;  // the state the stage starts from (uu, or the x filter's copy)
+    double *uu, *dudtRK;  // the updated state is written to uu
     double *spec;  // the context's dudt array: per-row scratch of d2/dy2 spectra
     // derivative arrays: doubles, or floats (field v at v * nx * ny) in the
     // mixed-precision stage
@@ -209,6 +210,7 @@ __global__ void __launch_bounds__(YR_THREADS, (YRGeom<L, T>::MINB)) yrow_kernel(
         return base ? reinterpret_cast<const T *>(base) + (size_t)v * plane + ro : nullptr;
     };
     auto su = [&](int v) -> double * { return a.uu + (size_t)v * plane + ro; };
+    auto si = [&](int v) -> const double * { return a.uin + (size_t)v * plane + ro; };
     // the row shift of the FP32 operators (see yr_load)
     auto sh = [&](const double *r) -> double { return MIX && valid ? r[0] : 0.0; };
 
@@ -219,7 +221,7 @@ __global__ void __launch_bounds__(YR_THREADS, (YRGeom<L, T>::MINB)) yrow_kernel(
     for (int q = 0; q < (a.mode == 2 ? 0 : npair); q++) {
         const int fa = q == 0 ? UX : q == 1 ? RHO : q == 2 ? UZ : q == 3 ? BX : PSI;
         const int fb = q == 0 ? UY : q == 1 ? P : q == 2 ? BZ : q == 3 ? BY : -1;
-        const double *ra = su(fa), *rb = fb >= 0 ? su(fb) : nullptr;
+        const double *ra = si(fa), *rb = fb >= 0 ? si(fb) : nullptr;
         const double ca = sh(ra), cb = rb ? sh(rb) : 0.0;
         T *o2a = nullptr, *o2b = nullptr;
         if (fa == UX && a.d2u) { o2a = f(a.d2udy2, 0); o2b = f(a.d2udy2, 1); }
@@ -251,7 +253,7 @@ __global__ void __launch_bounds__(YR_THREADS, (YRGeom<L, T>::MINB)) yrow_kernel(
         // flows) stays exactly zero here too, instead of picking up the
         // rounding of its partner in the packed complex transform.
         auto efield = [&](size_t o, double &ex, double &ey, double &ez) {
-            const double *u = a.uu + o;
+            const double *u = a.uin + o;
             double ux = u[UX * plane], uy = u[UY * plane], uz = u[UZ * plane];
             double bx = u[BX * plane], by = u[BY * plane], bz = u[BZ * plane];
             ex = uz * by - uy * bz;
@@ -310,7 +312,7 @@ __global__ void __launch_bounds__(YR_THREADS, (YRGeom<L, T>::MINB)) yrow_kernel(
 #pragma unroll
             for (int v = 0; v < 9; v++) {
                 if (v < nv) {
-                    u[v] = (T)a.uu[v * plane + o];
+                    u[v] = (T)a.uin[v * plane + o];
                     dx[v] = dudx[v * plane + o];
                     dy[v] = dudy[v * plane + o];
                 } else {
@@ -335,7 +337,7 @@ __global__ void __launch_bounds__(YR_THREADS, (YRGeom<L, T>::MINB)) yrow_kernel(
                     const double rv = (double)r[v];
                     // the FP64 state: re-read in FP32 mode (an L1 hit), the
                     // value already held in FP64 mode
-                    const double ud = MIX ? a.uu[v * plane + o] : (double)u[v];
+                    const double ud = MIX ? a.uin[v * plane + o] : (double)u[v];
                     a.uu[v * plane + o] = ud + cc * rv + dd * rk;
                     if (a.write_rk) a.dudtRK[v * plane + o] = rv;
                 }
@@ -398,6 +400,7 @@ int launch_yrow(Ctx *c, int iRK, int last_stage, int mode)
 {
     const mhdgpu_params &p = c->p;
     YRArgs a;
+    a.uin = state_ptr(c);
     a.uu = c->arr[MHDGPU_UU];
     a.dudtRK = c->arr[MHDGPU_DUDTRK];
     a.spec = c->arr[MHDGPU_DUDT];  // unused by the fused stage otherwise

@@ -51,7 +51,7 @@ PRECISION_FP64 = 0
 PRECISION_MIXED = 1
 
 # kernel classes of mhdgpu_profile_read
-KCLASSES = ("xsolve", "yspec", "pointwise", "reduce", "fused_x", "fused_y")
+KCLASSES = ("xsolve", "yspec", "pointwise", "reduce", "fused_x", "fused_y", "fused_xf")
 
 _lib = None
 
