@@ -145,7 +145,7 @@ __device__ __forceinline__ C twl(const C *__restrict__ tw, int m)
 // (t - k) R + k + r NS.  Thread j of the row's group does butterflies
 // j, j + N/16, ...  Two barriers: all reads complete before any write.
 // Twiddled passes (NS > 1) are radix 16 only.
-template <int N, int R, int NS, int SIGN, typename C>
+template <int N, int R, int NS, int SIGN, typename C, int TWS = 1>
 __device__ __forceinline__ void fft_pass(C *z, const C *__restrict__ tw, int j)
 {
     constexpr int T = N / 16;
@@ -167,7 +167,7 @@ __device__ __forceinline__ void fft_pass(C *z, const C *__restrict__ tw, int j)
     }
     if constexpr (NS > 1) {
         const int k = j & (NS - 1);
-        const int st = k * (N / (NS * 16));
+        const int st = k * (N / (NS * 16)) * TWS;
         // v[r + 8] takes W^{r+8} = W^r W^8: first the W^8 factor, then W^r
         // for both halves, so that few twiddles are live at a time
         const C w8 = twl<SIGN>(tw, 8 * st);
@@ -210,20 +210,22 @@ __device__ __forceinline__ void fft_pass(C *z, const C *__restrict__ tw, int j)
 }
 
 // In-place FFT of the padded row z (N = 2^L >= 16 points) by the N/16 threads
-// j = 0..N/16-1 of its group; every thread of the block must call it.
-template <int L, int SIGN, typename C>
+// j = 0..N/16-1 of its group; every thread of the block must call it.  The
+// twiddle table holds exp(-2 pi i m / (TWS N)) (TWS > 1: a table made for a
+// longer row).
+template <int L, int SIGN, typename C, int TWS = 1>
 __device__ __forceinline__ void fft_row(C *z, const C *__restrict__ tw, int j)
 {
     constexpr int N = 1 << L;
     static_assert(L >= 4 && L <= 13, "row length 16..8192");
     constexpr int REM = L % 4;
     constexpr int R0 = 1 << REM;  // the twiddle-free first pass (1: none)
-    if constexpr (REM == 1) fft_pass<N, 2, 1, SIGN>(z, tw, j);
-    if constexpr (REM == 2) fft_pass<N, 4, 1, SIGN>(z, tw, j);
-    if constexpr (REM == 3) fft_pass<N, 8, 1, SIGN>(z, tw, j);
-    fft_pass<N, 16, R0, SIGN>(z, tw, j);
-    if constexpr (L >= 8) fft_pass<N, 16, R0 * 16, SIGN>(z, tw, j);
-    if constexpr (L >= 12) fft_pass<N, 16, R0 * 256, SIGN>(z, tw, j);
+    if constexpr (REM == 1) fft_pass<N, 2, 1, SIGN, C, TWS>(z, tw, j);
+    if constexpr (REM == 2) fft_pass<N, 4, 1, SIGN, C, TWS>(z, tw, j);
+    if constexpr (REM == 3) fft_pass<N, 8, 1, SIGN, C, TWS>(z, tw, j);
+    fft_pass<N, 16, R0, SIGN, C, TWS>(z, tw, j);
+    if constexpr (L >= 8) fft_pass<N, 16, R0 * 16, SIGN, C, TWS>(z, tw, j);
+    if constexpr (L >= 12) fft_pass<N, 16, R0 * 256, SIGN, C, TWS>(z, tw, j);
 }
 
 }  // namespace mhd

@@ -185,6 +185,68 @@ __device__ __forceinline__ void yr_op12(const typename YRCplx<T>::C *tw, typenam
     __syncthreads();  // A may be refilled
 }
 
+// d/dy of one real row per half of the CTA (one CTA per row of N = 2^L
+// points), each through a complex FFT of M = N/2 points: the row's even
+// samples as the real part, the odd ones as the imaginary part.  The N-point
+// spectrum follows from the M-point one (X_k = A_k + W^k B_k and X_{k+M} =
+// A_k - W^k B_k, A and B the spectra of the even and odd samples, W =
+// exp(-2 pi i / N)); it is multiplied by the d/dy symbol and folded back the
+// same way for the inverse M-point FFT.  Each field is transformed alone, as
+// the reference's real transforms do, so a field that is zero stays exactly
+// zero.  get(g, i): sample i of the half's field g; put(g, i, v) stores the
+// result.  Ends with the block synchronised.
+template <int L, typename T, class Get, class Put>
+__device__ __forceinline__ void yr_real_pair(typename YRCplx<T>::C *Abase,
+                                             const typename YRCplx<T>::C *tw,
+                                             const typename YRCplx<T>::C *s1, Get get, Put put)
+{
+    using C = typename YRCplx<T>::C;
+    constexpr int N = 1 << L, M = N / 2, TH = M / 16;
+    static_assert(TH * 2 == YRGeom<L, T>::T_, "one row per CTA, two halves");
+    const int g = threadIdx.x / TH, jj = threadIdx.x % TH;
+    C *Z = Abase + (size_t)g * (M + M / 16);
+#pragma unroll
+    for (int m = 0; m < 16; m++) {
+        const int n = jj + m * TH;
+        Z[fpad(n)] = cmk<C>(get(g, 2 * n), get(g, 2 * n + 1));
+    }
+    __syncthreads();
+    fft_row<L - 1, -1, C, 2>(Z, tw, jj);
+    C zk[16], zm[16];
+#pragma unroll
+    for (int m = 0; m < 16; m++) {
+        const int k = jj + m * TH;
+        zk[m] = Z[fpad(k)];
+        zm[m] = Z[fpad((M - k) & (M - 1))];
+    }
+    __syncthreads();
+    using R = creal_t<C>;
+    const R h = (R)0.5;
+#pragma unroll
+    for (int m = 0; m < 16; m++) {
+        const int k = jj + m * TH;
+        const C a = cmk<C>(h * (zk[m].x + zm[m].x), h * (zk[m].y - zm[m].y));   // (Z_k + conj Z_-k)/2
+        const C b = cmk<C>(h * (zk[m].y + zm[m].y), -h * (zk[m].x - zm[m].x));  // (Z_k - conj Z_-k)/(2i)
+        const C w = __ldg(tw + k);
+        const C wb = cm(w, b);
+        const C y0 = cm(__ldg(s1 + k), ca(a, wb));
+        const C y1 = cm(__ldg(s1 + k + M), cs(a, wb));
+        const C e = ca(y0, y1);
+        const C o = cm(cs(y0, y1), cmk<C>(w.x, -w.y));  // times exp(+2 pi i k / N)
+        Z[fpad(k)] = cmk<C>(e.x - o.y, e.y + o.x);       // e + i o
+    }
+    __syncthreads();
+    fft_row<L - 1, +1, C, 2>(Z, tw, jj);
+#pragma unroll
+    for (int m = 0; m < 16; m++) {
+        const int n = jj + m * TH;
+        const C z = Z[fpad(n)];
+        put(g, 2 * n, z.x);
+        put(g, 2 * n + 1, z.y);
+    }
+    __syncthreads();
+}
+
 template <int L, typename T>
 __global__ void __launch_bounds__(YR_THREADS, (YRGeom<L, T>::MINB)) yrow_kernel(YRArgs a)
 {
@@ -246,12 +308,13 @@ __global__ void __launch_bounds__(YR_THREADS, (YRGeom<L, T>::MINB)) yrow_kernel(
         }
     }
     if (a.mode != 2) {
-        // E = -u x B formed in FP64; d/dy of Ex and Ez.  Ex is transformed
-        // with Ey (whose d/dy is not needed) and Ez alone, so that the
-        // out-of-plane family (uz, Bz, Ex, Ey) never shares a transform with
-        // an in-plane field: a field the reference keeps exactly zero (2-D
-        // flows) stays exactly zero here too, instead of picking up the
-        // rounding of its partner in the packed complex transform.
+        // E = -u x B formed in FP64; d/dy of Ex and Ez.  Ex (out-of-plane
+        // family: uz, Bz, Ex, Ey) and Ez (in-plane) never share a transform,
+        // so that a field the reference keeps exactly zero (2-D flows) stays
+        // exactly zero here too instead of picking up the rounding of its
+        // partner: on rows of one CTA each goes through its own real
+        // transform (yr_real_pair, the cost of one packed pair); on shorter
+        // rows Ex is packed with Ey (whose d/dy is not needed) and Ez alone.
         auto efield = [&](size_t o, double &ex, double &ey, double &ez) {
             const double *u = a.uin + o;
             double ux = u[UX * plane], uy = u[UY * plane], uz = u[UZ * plane];
@@ -262,22 +325,37 @@ __global__ void __launch_bounds__(YR_THREADS, (YRGeom<L, T>::MINB)) yrow_kernel(
         };
         double cx = 0.0, cy = 0.0, cz = 0.0;
         if (MIX && valid) efield(ro, cx, cy, cz);
+        if constexpr (G::ROWS == 1 && L >= 5) {
+            // Ex and Ez as real rows, side by side (yr_real_pair)
+            T *ox = f(a.dEdy, 0), *oz = f(a.dEdy, 2);
+            yr_real_pair<L, T>(
+                Abase, tw, s1,
+                [&](int g, int i) -> T {
+                    double ex = 0.0, ey = 0.0, ez = 0.0;
+                    if (valid) efield(ro + i, ex, ey, ez);
+                    return g == 0 ? (T)(ex - cx) : (T)(ez - cz);
+                },
+                [&](int g, int i, T v) {
+                    if (valid) (g == 0 ? ox : oz)[i] = v;
+                });
+        } else {
 #pragma unroll 4
-        for (int m = 0; m < 16; m++) {
-            const int i = j + m * G::T_;
-            double ex = 0.0, ey = 0.0, ez = 0.0;
-            if (valid) efield(ro + i, ex, ey, ez);
-            A[fpad(i)] = cmk<C>((T)(ex - cx), (T)(ey - cy));
-        }
-        yr_op<L, T, false>(tw, A, j, valid, s1, f(a.dEdy, 0), (T *)nullptr);
+            for (int m = 0; m < 16; m++) {
+                const int i = j + m * G::T_;
+                double ex = 0.0, ey = 0.0, ez = 0.0;
+                if (valid) efield(ro + i, ex, ey, ez);
+                A[fpad(i)] = cmk<C>((T)(ex - cx), (T)(ey - cy));
+            }
+            yr_op<L, T, false>(tw, A, j, valid, s1, f(a.dEdy, 0), (T *)nullptr);
 #pragma unroll 4
-        for (int m = 0; m < 16; m++) {
-            const int i = j + m * G::T_;
-            double ex = 0.0, ey = 0.0, ez = 0.0;
-            if (valid) efield(ro + i, ex, ey, ez);
-            A[fpad(i)] = cmk<C>((T)(ez - cz), (T)0);
+            for (int m = 0; m < 16; m++) {
+                const int i = j + m * G::T_;
+                double ex = 0.0, ey = 0.0, ez = 0.0;
+                if (valid) efield(ro + i, ex, ey, ez);
+                A[fpad(i)] = cmk<C>((T)(ez - cz), (T)0);
+            }
+            yr_op<L, T, false>(tw, A, j, valid, s1, f(a.dEdy, 2), (T *)nullptr);
         }
-        yr_op<L, T, false>(tw, A, j, valid, s1, f(a.dEdy, 2), (T *)nullptr);
     }
 
     if (a.mode == 1) return;  // uniform across the grid
