@@ -135,8 +135,10 @@ int mhdgpu_set_precision(mhdgpu_ctx *ctx, int precision);
  * shape created later in this process (a shape already tuned in this
  * process keeps its width, so runs repeat bit for bit).  The state is only
  * read; the derivative arrays are overwritten.  *columns_out: the width
- * chosen (may be NULL).  MHDGPU_ERR_UNSUPPORTED when the grid has no fused x
- * pass. */
+ * chosen (may be NULL); 0 when the context takes the chunked x pass (lines
+ * of 1024 rows and more), which has no width to choose and was measured
+ * faster than every width of the cluster pass there.
+ * MHDGPU_ERR_UNSUPPORTED when the grid has no fused x pass. */
 int mhdgpu_autotune(mhdgpu_ctx *ctx, int *columns_out);
 
 /* --- diagnostics -------------------------------------------------------- */

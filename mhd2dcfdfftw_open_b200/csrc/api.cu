@@ -589,6 +589,10 @@ extern "C" int mhdgpu_autotune(mhdgpu_ctx *h, int *columns_out)
 {
     CTX_OR_FAIL(h);
     if (settle(c)) return mhdgpu_last_error();
+    if (c->xn_on) {  // the chunked x pass: no tile width to choose
+        if (columns_out) *columns_out = 0;
+        return MHDGPU_OK;
+    }
     TRY(mhd::xline_autotune(c, columns_out));
     // the captured steps hold the previous tiling
     std::lock_guard<std::mutex> lock(g_device_mu);

@@ -27,6 +27,7 @@
 // The line values enter the dot products as differences to a nearby value u_c
 // (plus u_c times the sum of the taps), which keeps the rounding of the
 // inflow at the size of the line's variation, not of its mean.
+#include <algorithm>
 #include <cmath>
 #include <cstdlib>
 #include <cstring>
@@ -226,16 +227,19 @@ static int build_set(Ctx *c, XNHost *h, const XHostFactors &F, const int *ops, c
     constexpr int K = NT - 6;
     const long n = c->nx;
     const long nch = (n + L - 1) / L;
-    // the canonical interior chunk: in the middle of the line
+    // the canonical interior chunk: in the middle of the line; on lines too
+    // short to have one every chunk takes its own functionals from the table
     const long rc = (n / 2 / L) * L;
-    if (rc - K - 3 < XF_EDGE || rc + L + K + 3 > n - XF_EDGE) return MHDGPU_ERR_UNSUPPORTED;
+    const bool has_interior = rc - K - 3 >= XF_EDGE && rc + L + K + 3 <= n - XF_EDGE;
     const double m = F.m[n / 2], ib = F.ib[n / 2], g = F.g[n / 2];
     // the truncation: the dropped weights are below 2^-60 of the kept ones
+    // (the factors of the middle row are the interior limit on long lines
+    // and decay no slower than it on short ones)
     if (std::pow(std::fabs(m), K) >= std::ldexp(1.0, -60) ||
         std::pow(std::fabs(g), K) >= std::ldexp(1.0, -60))
         return MHDGPU_ERR_UNSUPPORTED;
     std::vector<XNRounded> cf(ns), cb(ns);
-    for (int s = 0; s < ns; s++) {
+    for (int s = 0; has_interior && s < ns; s++) {
         cf[s] = round_fun(fwd_fun(c, F, ops[s], delta[s], rc, K));
         cb[s] = round_fun(bwd_fun(c, F, ops[s], delta[s], rc + L, K));
         if ((int)cf[s].h.size() != NT || (int)cb[s].h.size() != NT || cf[s].j0 != rc - K - 3 ||
@@ -255,7 +259,7 @@ static int build_set(Ctx *c, XNHost *h, const XHostFactors &F, const int *ops, c
     for (long ci = 0; ci < nch; ci++) {
         const long r0 = ci * L, r1 = std::min(n, r0 + L);
         std::vector<XNRounded> ff(ns), fb(ns);
-        bool interior = r1 - r0 == L && r0 >= 3 && r1 + 3 <= n;
+        bool interior = has_interior && r1 - r0 == L && r0 >= 3 && r1 + 3 <= n;
         for (long r = r0; interior && r < r1; r++)
             interior = std::memcmp(&F.m[r], &m, sizeof m) == 0 &&
                        std::memcmp(&F.ib[r], &ib, sizeof ib) == 0 &&
@@ -581,12 +585,22 @@ __global__ void __launch_bounds__(32 * NW) xf_kernel(const __grid_constant__ XFP
 constexpr int XN_NW = 4;
 constexpr int XN_LD = 16;  // rows per chunk of the derivative kernel
 constexpr int XN_LF = 32;  // rows per chunk of the filter kernel
-constexpr long XN_MIN_NX = 1024;  // shorter lines keep the cluster x pass (xline.cu)
+// Lines shorter than this keep the cluster x pass (xline.cu), which holds a
+// whole short line in one CTA with no redundant work; MHDGPU_XN_MIN_NX sets
+// another bound (the chunked pass needs nx >= 2 chunks of XN_LF rows).
+// Measured on one B200: a job alone steps faster with the chunked pass from
+// 128^2 up (0.61 vs 1.66 ms per step at 128^2, 1.29 vs 1.68 ms at 512^2),
+// but the inflow dot products cost more work per cell on short lines, and
+// the 64-job ensemble served concurrently (the GPU full) runs 8 % faster
+// with the cluster pass below 1024 rows (335 M vs 310 M cell-updates/s).
+constexpr long XN_MIN_NX = 1024;
 
 int xn_setup(Ctx *c)
 {
     c->xn_on = 0;
-    if (c->nx < XN_MIN_NX || getenv("MHDGPU_NO_XN")) return MHDGPU_OK;
+    long min_nx = XN_MIN_NX;
+    if (const char *e = getenv("MHDGPU_XN_MIN_NX")) min_nx = std::max(2L * XN_LF, atol(e));
+    if (c->nx < min_nx || getenv("MHDGPU_NO_XN")) return MHDGPU_OK;
     XNHost *h = new (std::nothrow) XNHost();
     if (!h) return mhd_set_error(MHDGPU_ERR_NOMEM);
     std::memset(&h->d, 0, sizeof h->d);

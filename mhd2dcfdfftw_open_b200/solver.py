@@ -243,7 +243,7 @@ class Domain:
     def autotune(self):
         """Pick the fastest tile width of the fused x pass for this grid and
         precision (remembered for later domains of the same shape); returns
-        the width."""
+        the width, 0 for the chunked x pass of lines of 1024 rows and more."""
         w = ctypes.c_int(0)
         self._check(self.lib.mhdgpu_autotune(self.h, ctypes.byref(w)))
         return w.value

@@ -126,7 +126,7 @@ def test_autotune_keeps_the_results(nx, ny):
     p, uu = ic.alfvenic_turbulence(nx, ny, mmax=8)
     with Domain(p, uu) as a, Domain(p, uu) as b:
         w = b.autotune()
-        assert w in (8, 16, 32)
+        assert w in (0, 8, 16, 32)  # 0: the chunked x pass
         a.steps(3, 2e-4, fused=True)
         b.steps(3, 2e-4, fused=True)
         assert rel_l2(b.get("uu"), a.get("uu")).max() < 1e-12

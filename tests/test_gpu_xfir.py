@@ -1,8 +1,9 @@
 """GPU: the chunked x pass of long lines (csrc/xfir.cu) against the
 reference and against the cluster x pass it replaces there.
 
-On lines of 1024 rows and more the fused steps take the x filter and the x
-derivatives from per-chunk Thomas solves whose inflows are truncated
+On lines of 1024 rows and more (any length >= 64 with MHDGPU_XN_MIN_NX) the
+fused steps take the x filter and the x derivatives from per-chunk Thomas
+solves whose inflows are truncated
 functionals of the line (weights dropped below 2^-60 of the kept ones).  The
 results must meet the same gates as every other path: one RK3 step within
 1e-12 per field of the reference built from its own sources, five steps
@@ -25,6 +26,7 @@ pytestmark = pytest.mark.gpu
 
 def _run(p, uu, nsteps, dt_fixed, xn=True, mixed=False):
     old = os.environ.pop("MHDGPU_NO_XN", None)
+    os.environ["MHDGPU_XN_MIN_NX"] = "64"  # the chunked pass on the short lines too
     if not xn:
         os.environ["MHDGPU_NO_XN"] = "1"
     try:
@@ -35,11 +37,13 @@ def _run(p, uu, nsteps, dt_fixed, xn=True, mixed=False):
             return d.get("uu"), dt
     finally:
         os.environ.pop("MHDGPU_NO_XN", None)
+        os.environ.pop("MHDGPU_XN_MIN_NX", None)
         if old is not None:
             os.environ["MHDGPU_NO_XN"] = old
 
 
-@pytest.mark.parametrize("nx,ny", [(1024, 64), (1030, 32), (2048, 16)])
+@pytest.mark.parametrize("nx,ny", [(128, 128), (200, 64), (512, 256), (1024, 64), (1030, 32),
+                                   (2048, 16)])
 def test_one_step_vs_reference(reference, nx, ny):
     p, uu = ic.alfvenic_turbulence(nx, ny, mmax=min(8, ny // 4))
     reference.setup(p)
