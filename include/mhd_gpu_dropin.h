@@ -10,10 +10,10 @@
  * divBcleaning.c, links against this layer unchanged in place of
  * calcDerivs.o, calcRHS.o, filtering.o, timeAdvance.o and parallel.o.
  *
- * Every call copies the global arrays it reads to the device and the arrays
- * it writes back to the host, so the host globals always hold what the
- * reference would hold (checkDivB and writeArray in mhd.c read them
- * directly).  The device work runs on one context created on the first call
+ * By default every call copies the global arrays it reads to the device and
+ * the arrays it writes back to the host, so the host globals always hold
+ * what the reference would hold (checkDivB and writeArray in mhd.c read them
+ * directly).  Resident mode (below) keeps the arrays on the device instead.  The device work runs on one context created on the first call
  * from the globals that initialize() set (device 0, or MHDGPU_DEVICE).
  * Errors: these functions return void as the reference's do; a failure is
  * reported once on stderr and by mhdgpu_last_error().  Periodic x boundary
@@ -48,6 +48,21 @@ double calcDt(double dt0);
 void sendrecvHaloPointsX(void);
 void sendrecvHaloPointsdivBX(void);
 void sendrecvHaloPointsEfieldX(void);
+
+/* Resident mode (no counterpart in the reference): 1 keeps the global arrays
+ * on the device between calls -- each array is uploaded on its first use
+ * only, results stay on the device and the halo exchanges become no-ops (the
+ * kernels wrap periodically); 0 returns to copying on every call (and first
+ * brings the host up to date).  MHDGPU_DROPIN_RESIDENT=1 in the environment
+ * turns it on before the first call.  A driver then calls
+ * mhdgpu_dropin_sync_host() before it reads globals itself (for mhd.c: before
+ * each checkDivB/writeArray), and mhdgpu_dropin_sync_device() after it writes
+ * globals itself once the run has started (they are uploaded again on next
+ * use).  Changing a parameter global re-creates the context from the host
+ * arrays: sync the host first. */
+void mhdgpu_dropin_resident(int on);
+void mhdgpu_dropin_sync_host(void);
+void mhdgpu_dropin_sync_device(void);
 
 #ifdef __cplusplus
 }

@@ -3,10 +3,14 @@
  *
  * The reference keeps its state in globals defined by its initialize.c
  * (declared in its initialize.h:11-69, `real` = double); this file declares
- * the ones it uses with the same names and types.  Each entry point uploads
- * the global arrays it reads, runs the operator of libmhdgpu.so on them, and
- * downloads the arrays it writes, so the host globals stay exactly what the
- * reference's own routines would leave there.
+ * the ones it uses with the same names and types.  By default each entry
+ * point uploads the global arrays it reads, runs the operator of
+ * libmhdgpu.so on them, and downloads the arrays it writes, so the host
+ * globals stay exactly what the reference's own routines would leave there.
+ * In resident mode (mhdgpu_dropin_resident, or MHDGPU_DROPIN_RESIDENT=1) the
+ * device copies are authoritative: each array crosses PCIe on its first use
+ * only, and results come back in mhdgpu_dropin_sync_host, which a driver
+ * calls before it reads the globals itself (mhd.c's checkDivB and writeArray).
  */
 #include <math.h>
 #include <stdio.h>
@@ -34,6 +38,22 @@ extern double *uuHaloX0, *uuHaloX1, *divBHaloX0, *divBHaloX1, *EfieldHaloX0, *Ef
 static mhdgpu_ctx *g_ctx = NULL;
 static mhdgpu_params g_p;  /* the parameters g_ctx was created with */
 static int g_reported = 0;
+
+/* Resident mode (mhdgpu_dropin_resident): the device arrays are the
+ * authoritative copy.  An array is uploaded on its first use only
+ * (g_uploaded), results stay on the device (g_dev_newer marks arrays whose
+ * host copy is stale) and reach the host in mhdgpu_dropin_sync_host. */
+static int g_resident = -1;  /* -1: not decided yet (MHDGPU_DROPIN_RESIDENT) */
+static unsigned char g_uploaded[MHDGPU_NARRAYS], g_dev_newer[MHDGPU_NARRAYS];
+
+static int resident(void)
+{
+    if (g_resident < 0) {
+        const char *e = getenv("MHDGPU_DROPIN_RESIDENT");
+        g_resident = e && atoi(e) != 0;
+    }
+    return g_resident;
+}
 
 static void report(const char *where, int rc)
 {
@@ -76,6 +96,9 @@ static mhdgpu_ctx *ctx(void)
     if (g_ctx && same_params(&p, &g_p)) return g_ctx;
     if (g_ctx) mhdgpu_destroy(g_ctx);
     g_ctx = NULL;
+    /* a new context starts from the host globals */
+    memset(g_uploaded, 0, sizeof g_uploaded);
+    memset(g_dev_newer, 0, sizeof g_dev_newer);
     const char *dev = getenv("MHDGPU_DEVICE");
     int rc = mhdgpu_create(&p, dev ? atoi(dev) : 0, &g_ctx);
     if (rc != MHDGPU_OK) {
@@ -109,14 +132,45 @@ static int up(mhdgpu_ctx *c, int k)
 {
     double *h = host_of(k);
     if (!h || !mhdgpu_device_array(c, k)) return MHDGPU_OK;  /* not allocated: not used */
-    return mhdgpu_set_array(c, k, h);
+    if (resident() && (g_uploaded[k] || g_dev_newer[k])) return MHDGPU_OK;
+    int rc = mhdgpu_set_array(c, k, h);
+    if (!rc) g_uploaded[k] = 1;
+    return rc;
 }
 
 static int down(mhdgpu_ctx *c, int k)
 {
     double *h = host_of(k);
     if (!h || !mhdgpu_device_array(c, k)) return MHDGPU_OK;
+    if (resident()) {
+        g_dev_newer[k] = 1;
+        return MHDGPU_OK;
+    }
     return mhdgpu_get_array(c, k, h);
+}
+
+void mhdgpu_dropin_resident(int on)
+{
+    if (resident() && !on) mhdgpu_dropin_sync_host();
+    g_resident = on != 0;
+}
+
+void mhdgpu_dropin_sync_host(void)
+{
+    if (!g_ctx) return;
+    for (int k = 0; k < MHDGPU_NARRAYS; k++) {
+        if (!g_dev_newer[k]) continue;
+        double *h = host_of(k);
+        int rc = h && mhdgpu_device_array(g_ctx, k) ? mhdgpu_get_array(g_ctx, k, h) : MHDGPU_OK;
+        report("mhdgpu_dropin_sync_host", rc);
+        if (!rc) g_dev_newer[k] = 0;
+    }
+}
+
+void mhdgpu_dropin_sync_device(void)
+{
+    memset(g_uploaded, 0, sizeof g_uploaded);
+    memset(g_dev_newer, 0, sizeof g_dev_newer);
 }
 
 static void deriv(const char *name, int dir, int order, int nv, double *in, int start,
@@ -211,8 +265,14 @@ void rkInit(double dt)
 {
     mhdgpu_ctx *c = ctx();
     if (!c) return;
-    memset(dudtRK, 0, sizeof(double) * (size_t)NVAR * iSize * jSize);
-    report("rkInit", mhdgpu_rk_init(c, dt));
+    int rc = mhdgpu_rk_init(c, dt);
+    if (resident()) {  /* zeroed on the device, which is authoritative */
+        g_uploaded[MHDGPU_DUDTRK] = 1;
+        g_dev_newer[MHDGPU_DUDTRK] = 1;
+    } else {
+        memset(dudtRK, 0, sizeof(double) * (size_t)NVAR * iSize * jSize);
+    }
+    report("rkInit", rc);
 }
 
 void rkExecute(int iRK)
@@ -261,6 +321,17 @@ static void halo(const double *a, int nf, double *h0, double *h1)
         }
 }
 
-void sendrecvHaloPointsX(void) { halo(uu, NVAR, uuHaloX0, uuHaloX1); }
-void sendrecvHaloPointsdivBX(void) { halo(divB, 1, divBHaloX0, divBHaloX1); }
-void sendrecvHaloPointsEfieldX(void) { halo(Efield, 3, EfieldHaloX0, EfieldHaloX1); }
+/* In resident mode the host arrays are stale between syncs; the kernels wrap
+ * periodically and never read these halos, so they are left alone. */
+void sendrecvHaloPointsX(void)
+{
+    if (!resident()) halo(uu, NVAR, uuHaloX0, uuHaloX1);
+}
+void sendrecvHaloPointsdivBX(void)
+{
+    if (!resident()) halo(divB, 1, divBHaloX0, divBHaloX1);
+}
+void sendrecvHaloPointsEfieldX(void)
+{
+    if (!resident()) halo(Efield, 3, EfieldHaloX0, EfieldHaloX1);
+}

@@ -89,9 +89,11 @@ def test_initial_conditions():
     assert all(b.arrival > a.arrival for a, b in zip(reqs, reqs[1:]))
 
 
-def _declared_functions():
+def _declared_functions(headers=("mhd_gpu.h",)):
+    """Functions declared in the C-ABI headers (mhd_gpu.h: libmhdgpu.so;
+    mhd_gpu_dropin.h: the drop-in archive, checked below)."""
     names = []
-    for h in ("mhd_gpu.h", "mhd_gpu_dropin.h"):
+    for h in headers:
         path = os.path.join(ROOT, "include", h)
         if not os.path.exists(path):
             continue
