@@ -52,9 +52,8 @@ struct XHostFactors {
 
 // Weights of the right-hand side of operator `op` at row gr on u(gr-3..gr+3)
 // (mathlib.c:46-85, 176-217, 309-353; unwrapped indices, the periodic wrap
-// is applied when the line is read).  delta: the filter's change system
-// (B - A) of the mixed-precision filter.
-static void rhs_weights(const Ctx *c, int op, bool delta, long gr, long n, long double w[7])
+// is applied when the line is read).
+static void rhs_weights(const Ctx *c, int op, long gr, long n, long double w[7])
 {
     const XStencil &s = c->xs[op];
     const long double sc = s.scale;
@@ -73,13 +72,6 @@ static void rhs_weights(const Ctx *c, int op, bool delta, long gr, long n, long 
     } else {
         w[0] = w[6] = s.d; w[1] = w[5] = s.c; w[2] = w[4] = s.b; w[3] = s.a;
     }
-    if (delta) {  // minus the filter matrix row (initTriMatrixCFDFilter)
-        const long double lo = gr == 0 ? 0.0L : (gr == n - 1 ? c->xf_alphaF[1] : c->xf_alphaF[0]);
-        const long double up = gr == n - 1 ? 0.0L : (gr == 0 ? c->xf_alphaF[1] : c->xf_alphaF[0]);
-        w[2] -= lo;
-        w[3] -= 1.0L;
-        w[4] -= up;
-    }
 }
 
 // A functional sum_j h_j u(j0 + j) (j = 0..h.size()-1), plus the constant A
@@ -91,11 +83,11 @@ struct XNFun {
 };
 
 // add weight `p` times the right-hand side of row k to f
-static void add_row(const Ctx *c, int op, bool delta, long k, long n, long double p,
+static void add_row(const Ctx *c, int op, long k, long n, long double p,
                     std::map<long, long double> &acc)
 {
     long double w[7];
-    rhs_weights(c, op, delta, k, n, w);
+    rhs_weights(c, op, k, n, w);
     for (int s = 0; s < 7; s++)
         if (w[s] != 0.0L) acc[k - 3 + s] += p * w[s];
 }
@@ -113,13 +105,13 @@ static XNFun to_fun(const std::map<long, long double> &acc)
 
 // y(r0 - 1) as a functional of the line, the sum truncated after K rows
 // (exact when the line starts within them)
-static XNFun fwd_fun(const Ctx *c, const XHostFactors &F, int op, bool delta, long r0, int K)
+static XNFun fwd_fun(const Ctx *c, const XHostFactors &F, int op, long r0, int K)
 {
     const long n = c->nx;
     std::map<long, long double> acc;
     long double P = 1.0L;
     for (long k = r0 - 1; k >= 0 && k >= r0 - K; k--) {
-        add_row(c, op, delta, k, n, P, acc);
+        add_row(c, op, k, n, P, acc);
         P *= -(long double)F.m[k];
     }
     return to_fun(acc);
@@ -127,7 +119,7 @@ static XNFun fwd_fun(const Ctx *c, const XHostFactors &F, int op, bool delta, lo
 
 // x(r1) = A y(r1 - 1) + functional of the line, truncated after K rows
 // (exact when the line ends within them)
-static XNFun bwd_fun(const Ctx *c, const XHostFactors &F, int op, bool delta, long r1, int K)
+static XNFun bwd_fun(const Ctx *c, const XHostFactors &F, int op, long r1, int K)
 {
     const long n = c->nx;
     const long kmax = std::min(n - 1, r1 + (long)K - 1);
@@ -146,7 +138,7 @@ static XNFun bwd_fun(const Ctx *c, const XHostFactors &F, int op, bool delta, lo
         cc[(size_t)(i - r1)] = run;
     }
     std::map<long, long double> acc;
-    for (long i = r1; i <= kmax; i++) add_row(c, op, delta, i, n, cc[(size_t)(i - r1)], acc);
+    for (long i = r1; i <= kmax; i++) add_row(c, op, i, n, cc[(size_t)(i - r1)], acc);
     XNFun f = to_fun(acc);
     f.A = -(long double)F.m[r1] * cc[0];
     return f;
@@ -198,7 +190,7 @@ static int host_factors(const Ctx *c, int op, XHostFactors &F)
 // tables they point to.
 struct XNHost {
     XDParams d;
-    XFParams f, fd;  // FP64 filter; change system of the mixed-precision filter
+    XFParams f;
     std::vector<void *> dev;
 };
 
@@ -221,8 +213,8 @@ static int dev_copy(XNHost *h, const std::vector<T> &v, const T **out)
 // when the line is too short to have interior chunks or the interior factors
 // do not decay below 2^-60 within K rows.
 template <int NT>
-static int build_set(Ctx *c, XNHost *h, const XHostFactors &F, const int *ops, const bool *delta,
-                     int ns, int L, XNTaps<NT> *inner, XNCommon &k)
+static int build_set(Ctx *c, XNHost *h, const XHostFactors &F, const int *ops, int ns, int L,
+                     XNTaps<NT> *inner, XNCommon &k)
 {
     constexpr int K = NT - 6;
     const long n = c->nx;
@@ -240,8 +232,8 @@ static int build_set(Ctx *c, XNHost *h, const XHostFactors &F, const int *ops, c
         return MHDGPU_ERR_UNSUPPORTED;
     std::vector<XNRounded> cf(ns), cb(ns);
     for (int s = 0; has_interior && s < ns; s++) {
-        cf[s] = round_fun(fwd_fun(c, F, ops[s], delta[s], rc, K));
-        cb[s] = round_fun(bwd_fun(c, F, ops[s], delta[s], rc + L, K));
+        cf[s] = round_fun(fwd_fun(c, F, ops[s], rc, K));
+        cb[s] = round_fun(bwd_fun(c, F, ops[s], rc + L, K));
         if ((int)cf[s].h.size() != NT || (int)cb[s].h.size() != NT || cf[s].j0 != rc - K - 3 ||
             cb[s].j0 != rc + L - 3)
             return MHDGPU_ERR_UNSUPPORTED;
@@ -265,8 +257,8 @@ static int build_set(Ctx *c, XNHost *h, const XHostFactors &F, const int *ops, c
                        std::memcmp(&F.ib[r], &ib, sizeof ib) == 0 &&
                        std::memcmp(&F.g[r], &g, sizeof g) == 0;
         for (int s = 0; s < ns; s++) {
-            ff[s] = round_fun(r0 > 0 ? fwd_fun(c, F, ops[s], delta[s], r0, K) : XNFun{});
-            fb[s] = round_fun(r1 < n ? bwd_fun(c, F, ops[s], delta[s], r1, K) : XNFun{});
+            ff[s] = round_fun(r0 > 0 ? fwd_fun(c, F, ops[s], r0, K) : XNFun{});
+            fb[s] = round_fun(r1 < n ? bwd_fun(c, F, ops[s], r1, K) : XNFun{});
             interior = interior && same_fun(ff[s], cf[s], r0 - rc) && same_fun(fb[s], cb[s], r0 - rc);
         }
         if (interior) continue;
@@ -342,23 +334,20 @@ struct XNEfield {
 };
 
 // Thomas solve of one chunk, rows r0 .. r0+len-1, for NS systems sharing the
-// factors in k: system s applies operator OPS[s] to input INS[s] of `in`
-// (delta: the filter's change system, FP64 right-hand side minus the matrix
-// row), with the interior taps tp0/tp1 or, for an edge chunk (e >= 0), the
+// factors in k: system s applies operator OPS[s] to input INS[s] of `in`, with the interior taps tp0/tp1 or, for an edge chunk (e >= 0), the
 // table entries k.edge[e + E1 * s].  The recurrences run in T.  Results x go to
 // emit(s, row, x).
-template <int L, typename T, int NS, int NT, int OP0, int OP1, int IN1, int E1, bool DELTA, int UNR,
-          class In, class Emit>
+template <int L, typename T, int NS, int NT, int OP0, int OP1, int IN1, int E1, int UNR, class In,
+          class Emit>
 __device__ __forceinline__ void xn_chunk(const XNCommon &k, const XNTaps<NT> &tp0,
                                          const XNTaps<NT> &tp1, const XStencil &st0,
-                                         const XStencil &st1, double fa_in, double fa_sub,
-                                         const In &in, long r0, int len, int e, Emit emit)
+                                         const XStencil &st1, const In &in, long r0, int len,
+                                         int e, Emit emit)
 {
     constexpr int NI = In::NI;
     constexpr int ops[2] = {OP0, OP1};
     constexpr int ins[2] = {0, IN1};
     constexpr int eo[2] = {0, E1};  // table entry of each system, from e
-    constexpr bool delta = DELTA;
 #define TP(s) ((s) == 0 ? tp0 : tp1)
 #define ST(s) ((s) == 0 ? st0 : st1)
     const long n = k.nx;
@@ -402,7 +391,6 @@ __device__ __forceinline__ void xn_chunk(const XNCommon &k, const XNTaps<NT> &tp
                 if (ops[s] == XOP_D1) rhs = xn_rhs<XOP_D1>(ST(s), x[0], x[1], x[2], x[3], x[4], x[5], x[6]);
                 else if (ops[s] == XOP_D2) rhs = xn_rhs<XOP_D2>(ST(s), x[0], x[1], x[2], x[3], x[4], x[5], x[6]);
                 else rhs = xn_rhs<XOP_F>(ST(s), x[0], x[1], x[2], x[3], x[4], x[5], x[6]);
-                if (delta) rhs -= fa_in * (x[2] + x[4]) + x[3];
                 y[s] = (T)rhs - m * y[s];
                 Y[s][r] = y[s];
             }
@@ -471,11 +459,6 @@ __device__ __forceinline__ void xn_chunk(const XNCommon &k, const XNTaps<NT> &tp
             for (int s = 0; s < NS; s++) {
                 const double *x = w[ins[s]];
                 double rhs = stencil(ST(s), x[0], x[1], x[2], x[3], x[4], x[5], x[6], gr, n);
-                if (delta) {
-                    const double lo = gr == 0 ? 0.0 : (gr == n - 1 ? fa_sub : fa_in);
-                    const double up = gr == n - 1 ? 0.0 : (gr == 0 ? fa_sub : fa_in);
-                    rhs -= lo * x[2] + x[3] + up * x[4];
-                }
                 y[s] = (T)rhs - m * y[s];
                 Y[s][r] = y[s];
             }
@@ -537,18 +520,18 @@ __global__ void __launch_bounds__(32 * NW) xd_kernel(const __grid_constant__ XDP
         else if (P.out2b && v >= P.d2b_lo && v < P.d2b_lo + 3)
             d2 = reinterpret_cast<T *>(P.out2b) + (size_t)(v - P.d2b_lo) * plane + j;
         if (d2)  // d/dx and d2/dx2 share the matrix: one pass over the line
-            xn_chunk<L, T, 2, XN_TD, XOP_D1, XOP_D2, 0, 1, false, UNR>(
-                P.k, P.s[0], P.s[1], P.st[0], P.st[1], 0.0, 0.0, in, r0, len, e,
+            xn_chunk<L, T, 2, XN_TD, XOP_D1, XOP_D2, 0, 1, UNR>(
+                P.k, P.s[0], P.s[1], P.st[0], P.st[1], in, r0, len, e,
                 [&](int s, long row, T x) { (s == 0 ? d1 : d2)[row * ny] = x; });
         else
-            xn_chunk<L, T, 1, XN_TD, XOP_D1, XOP_D1, 0, 0, false, UNR>(
-                P.k, P.s[0], P.s[0], P.st[0], P.st[0], 0.0, 0.0, in, r0, len, e,
+            xn_chunk<L, T, 1, XN_TD, XOP_D1, XOP_D1, 0, 0, UNR>(
+                P.k, P.s[0], P.s[0], P.st[0], P.st[0], in, r0, len, e,
                 [&](int, long row, T x) { d1[row * ny] = x; });
     } else {  // d/dx of Ey and Ez, formed from the state as the lines are read
         const XNEfield in{P.in + j, ny, plane};
         T *ey = reinterpret_cast<T *>(P.outE) + j, *ez = ey + plane;
-        xn_chunk<L, T, 2, XN_TD, XOP_D1, XOP_D1, 1, 0, false, UNR>(
-            P.k, P.s[0], P.s[0], P.st[0], P.st[0], 0.0, 0.0, in, r0, len, e,
+        xn_chunk<L, T, 2, XN_TD, XOP_D1, XOP_D1, 1, 0, UNR>(
+            P.k, P.s[0], P.s[0], P.st[0], P.st[0], in, r0, len, e,
             [&](int s, long row, T x) { (s == 0 ? ey : ez)[row * ny] = x; });
     }
 }
@@ -556,6 +539,7 @@ __global__ void __launch_bounds__(32 * NW) xd_kernel(const __grid_constant__ XDP
 template <int L, typename T, int UNR, int NW>
 __global__ void __launch_bounds__(32 * NW) xf_kernel(const __grid_constant__ XFParams P)
 {
+    static_assert(sizeof(T) == 8, "the x filter runs in FP64 in both precisions");
     const int lane = threadIdx.x & 31;
     const long j = (long)blockIdx.x * 32 + lane;
     const int ci = (int)blockIdx.y * NW + (int)(threadIdx.x >> 5);
@@ -567,14 +551,9 @@ __global__ void __launch_bounds__(32 * NW) xf_kernel(const __grid_constant__ XFP
     const int v = (int)blockIdx.z;
     const XNField in{P.in + (size_t)v * plane + j, ny};
     double *out = P.out + (size_t)v * plane + j;
-    if constexpr (sizeof(T) == 8)
-        xn_chunk<L, double, 1, XN_TF, XOP_F, XOP_F, 0, 0, false, UNR>(
-            P.k, P.s, P.s, P.st, P.st, 0.0, 0.0, in, r0, len, e,
-            [&](int, long row, double x) { out[row * ny] = x; });
-    else  // the change d of the line in FP32, added to the FP64 line
-        xn_chunk<L, float, 1, XN_TF, XOP_F, XOP_F, 0, 0, true, UNR>(
-            P.k, P.s, P.s, P.st, P.st, P.fa_in, P.fa_sub, in, r0, len, e,
-            [&](int, long row, float x) { out[row * ny] = in.p[row * ny] + (double)x; });
+    xn_chunk<L, double, 1, XN_TF, XOP_F, XOP_F, 0, 0, UNR>(
+        P.k, P.s, P.s, P.st, P.st, in, r0, len, e,
+        [&](int, long row, double x) { out[row * ny] = x; });
 }
 
 // ---------------------------------------------------------------------------
@@ -605,7 +584,6 @@ int xn_setup(Ctx *c)
     if (!h) return mhd_set_error(MHDGPU_ERR_NOMEM);
     std::memset(&h->d, 0, sizeof h->d);
     std::memset(&h->f, 0, sizeof h->f);
-    std::memset(&h->fd, 0, sizeof h->fd);
     c->xn = h;
     XHostFactors FD, FD2, FF;
     int rc;
@@ -615,8 +593,7 @@ int xn_setup(Ctx *c)
     if (FD.m != FD2.m || FD.ib != FD2.ib || FD.g != FD2.g) return MHDGPU_OK;  // not one matrix
     {
         const int ops[2] = {XOP_D1, XOP_D2};
-        const bool delta[2] = {false, false};
-        rc = build_set<XN_TD>(c, h, FD, ops, delta, 2, XN_LD, h->d.s, h->d.k);
+        rc = build_set<XN_TD>(c, h, FD, ops, 2, XN_LD, h->d.s, h->d.k);
         if (rc == MHDGPU_ERR_UNSUPPORTED) return MHDGPU_OK;
         if (rc) return rc;
         h->d.k.tm = c->xt[XOP_D1].m;
@@ -625,19 +602,16 @@ int xn_setup(Ctx *c)
         h->d.st[0] = c->xs[XOP_D1];
         h->d.st[1] = c->xs[XOP_D2];
     }
-    for (int k = 0; k < 2; k++) {
-        XFParams &f = k == 0 ? h->f : h->fd;
+    {
+        XFParams &f = h->f;
         const int ops[1] = {XOP_F};
-        const bool delta[1] = {k == 1};
-        rc = build_set<XN_TF>(c, h, FF, ops, delta, 1, XN_LF, &f.s, f.k);
+        rc = build_set<XN_TF>(c, h, FF, ops, 1, XN_LF, &f.s, f.k);
         if (rc == MHDGPU_ERR_UNSUPPORTED) return MHDGPU_OK;
         if (rc) return rc;
         f.k.tm = c->xt[XOP_F].m;
         f.k.tib = c->xt[XOP_F].invB;
         f.k.tg = c->xt[XOP_F].g;
         f.st = c->xs[XOP_F];
-        f.fa_in = c->xf_alphaF[0];
-        f.fa_sub = c->xf_alphaF[1];
     }
     const size_t plane = (size_t)c->nx * c->ny;
     MHD_CUDA_TRY(cudaMalloc(&c->xn_state, sizeof(double) * plane * c->nvar));
@@ -699,7 +673,12 @@ int launch_xf(Ctx *c, const double *in, double *out)
 {
     XNHost *h = static_cast<XNHost *>(c->xn);
     if (!c->xn_on || !h || in == out) return mhd_set_error(MHDGPU_ERR_INVALID);
-    XFParams P = c->mixed ? h->fd : h->f;
+    // Mixed precision too takes the FP64 filter: the inflow dot products are
+    // FP64 either way, and the FP32 change-system variant (d = A^-1 (B - A) u
+    // added to u) measured slower on B200 (2.04 vs 1.58 ms per launch at
+    // 4096^2: it spills at the fully unrolled taps); the FP64 filter is also
+    // the exact one.
+    XFParams P = h->f;
     P.in = in;
     P.out = out;
     const size_t plane = (size_t)c->nx * c->ny;
@@ -707,15 +686,9 @@ int launch_xf(Ctx *c, const double *in, double *out)
     dim3 grid((unsigned)((c->ny + 31) / 32), (unsigned)((P.k.nch + XN_NW - 1) / XN_NW),
               (unsigned)c->nvar);
     prof_begin(c, KC_FUSED_XF, bytes);
-#define XF_LAUNCH(U, W)                                                                          \
-    do {                                                                                         \
-        if (c->mixed) xf_kernel<XN_LF, float, U, W><<<grid, 32 * W, 0, c->stream>>>(P);          \
-        else xf_kernel<XN_LF, double, U, W><<<grid, 32 * W, 0, c->stream>>>(P);                  \
-    } while (0)
     // the inflow dot products fully unrolled: every tap's load in flight at
     // once (twice as fast on B200 as unrolling by 8)
-    XF_LAUNCH(XN_TF, XN_NW);
-#undef XF_LAUNCH
+    xf_kernel<XN_LF, double, XN_TF, XN_NW><<<grid, 32 * XN_NW, 0, c->stream>>>(P);
     prof_end(c);
     MHD_CHECK_LAUNCH();
     return MHDGPU_OK;

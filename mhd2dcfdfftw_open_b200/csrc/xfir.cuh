@@ -51,15 +51,13 @@ struct XDParams {
     int nvar, d2a_lo, d2b_lo;
 };
 
-// x filter of every field: out = F_x(in); in mixed precision the change
-// system (B - A) d = ... in FP32, added to the FP64 line.
+// x filter of every field: out = F_x(in), in FP64 in both precisions.
 struct XFParams {
     XNTaps<XN_TF> s;
     XStencil st;
     XNCommon k;
     const double *in;
     double *out;
-    double fa_in, fa_sub;         // filter matrix off-diagonals (change system)
 };
 
 int xn_setup(Ctx *c);
