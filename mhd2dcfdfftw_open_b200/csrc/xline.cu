@@ -590,15 +590,23 @@ xline_kernel(XFArgs a, const __grid_constant__ CUtensorMap tm_big,
     int par = 0;  // alternates the carry-exchange arrays between solves
     if (nf > 0 && tid < 32) xl_stage<W>(a, s, 0, a.in_start, r0, Rc, j0, &tm_big, &tm_unit);
 
+    // Block-uniform: set once a tile wait of this CTA ran out.  From then on
+    // the CTA issues no copy and waits on no barrier (the tile that never
+    // landed may still be in flight, so its buffer is not reused); it keeps
+    // solving on whatever the tiles hold so that every cluster barrier is
+    // still reached by every CTA, and the host reports MHDGPU_ERR_TIMEOUT.
+    int failed = 0;
     for (int f = 0; f < nf; f++) {
         const int b = f & 1;
         const int v = a.in_start + f;
         // the other tile is free: its last readers finished before the
         // cluster barriers of the previous field's solves
-        if (f + 1 < nf && tid < 32) xl_stage<W>(a, s, b ^ 1, v + 1, r0, Rc, j0, &tm_big, &tm_unit);
-        mbar_wait_bounded(&s.bar[b], phase[b], a.flag);
+        if (!failed && f + 1 < nf && tid < 32)
+            xl_stage<W>(a, s, b ^ 1, v + 1, r0, Rc, j0, &tm_big, &tm_unit);
+        bool ok = true;
+        if (!failed) ok = mbar_wait_bounded(&s.bar[b], phase[b], a.flag);
         phase[b] ^= 1u;
-        __syncthreads();
+        failed = __syncthreads_or(failed || !ok);
         double *t = s.tile[b];
         if (a.single_op >= 0) {  // one operator per field
             const size_t off = (size_t)f * plane + j0 + lane;
