@@ -123,7 +123,7 @@ int mhdgpu_steps_fused(mhdgpu_ctx *ctx, int nsteps, double dt_fixed, double *dt_
  * filters are applied as an FP32 change added to the FP64 state.  After
  * mixed steps the derivative arrays hold FP32 scratch (mhdgpu_check_divb then
  * returns MHDGPU_ERR_UNSUPPORTED until an FP64 step has run).  Mixed
- * precision needs the fused path: 16 <= ny <= 4096, a grid the fused x pass
+ * precision needs the fused path: 16 <= ny <= 8192, a grid the fused x pass
  * tiles, and divBcleaning 0 or 2; otherwise MHDGPU_ERR_UNSUPPORTED. */
 enum { MHDGPU_PRECISION_FP64 = 0, MHDGPU_PRECISION_MIXED = 1 };
 int mhdgpu_set_precision(mhdgpu_ctx *ctx, int precision);

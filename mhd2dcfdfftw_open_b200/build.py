@@ -7,6 +7,7 @@ nvcc for sm_100a (``-gencode arch=compute_100a,code=sm_100a``) into
 """
 from __future__ import annotations
 
+import concurrent.futures
 import glob
 import os
 import shutil
@@ -47,15 +48,19 @@ def build(force: bool = False, verbose: bool = False) -> str:
     cus = sorted(glob.glob(os.path.join(CSRC, "*.cu")))
     hdrs = sorted(glob.glob(os.path.join(CSRC, "*.cuh")) +
                   glob.glob(os.path.join(ROOT, "include", "*.h")))
-    objs = []
+    objs, cmds = [], []
     for cu in cus:
         obj = os.path.join(BUILD_DIR, os.path.basename(cu) + ".o")
         objs.append(obj)
         if force or _stale(obj, [cu] + hdrs):
-            cmd = [nvcc()] + NVCC_FLAGS + ["-dc", cu, "-o", obj]
+            cmds.append([nvcc()] + NVCC_FLAGS + ["-dc", cu, "-o", obj])
+    # the translation units are independent: compile them side by side
+    with concurrent.futures.ThreadPoolExecutor(max(1, min(len(cmds), os.cpu_count() or 1))) as ex:
+        for cmd in cmds:
             if verbose:
                 print(" ".join(cmd))
-            subprocess.run(cmd, check=True)
+        for f in [ex.submit(subprocess.run, cmd, check=True) for cmd in cmds]:
+            f.result()
     if force or _stale(LIB, objs):
         cmd = [nvcc(), "-gencode", "arch=compute_100a,code=sm_100a", "-shared",
                "-Xcompiler", "-fPIC", "-o", LIB] + objs + ["-lcudart"]

@@ -486,7 +486,7 @@ static int fused_step_dev(Ctx *c, bool need_dt, bool keep_dt)
 // tile (an odd nx with 8 columns), and diffusive cleaning (divBcleaning == 1)
 // where the y row kernel does not apply, run through the operator stage.
 //
-// With the row kernel (16 <= ny <= 4096) the step control stays on the
+// With the row kernel (16 <= ny <= 8192) the step control stays on the
 // device: dt (and Ch, Cp) live in dscal, the y pass forms cc = c_k dt and
 // dd = d_k dt there, calcDt runs on the device (the reference's arithmetic
 // and hysteresis, timeAdvance.c:38-153), and dudtRK needs no clearing between

@@ -64,12 +64,14 @@ struct YRGeom {
     static constexpr int N = 1 << L;
     static constexpr int T_ = N / 16;                                   // threads per row
     static constexpr int ROWS = T_ >= YR_THREADS ? 1 : YR_THREADS / T_;  // rows per CTA
+    // threads per CTA: YR_THREADS, or one row of 8192 points by 512 threads
+    static constexpr int THREADS = T_ * ROWS;
     static constexpr int NP = N + N / 16;                              // padded row
     // shared memory: one padded FFT row per row of the CTA (68 KB in FP64,
-    // 34 KB in FP32, for any row length)
+    // 34 KB in FP32, for rows up to 4096 points; twice that for 8192)
     static constexpr size_t SMEM = sizeof(C) * ROWS * NP;
     // CTAs per SM the register budget is set for
-    static constexpr int MINB = sizeof(T) == 8 ? 2 : 3;
+    static constexpr int MINB = THREADS > YR_THREADS ? 1 : (sizeof(T) == 8 ? 2 : 3);
 };
 
 // Load fields fa and fb (fb < 0: zero) of this group's row into the FFT row
@@ -248,7 +250,7 @@ __device__ __forceinline__ void yr_real_pair(typename YRCplx<T>::C *Abase,
 }
 
 template <int L, typename T>
-__global__ void __launch_bounds__(YR_THREADS, (YRGeom<L, T>::MINB)) yrow_kernel(YRArgs a)
+__global__ void __launch_bounds__((YRGeom<L, T>::THREADS), (YRGeom<L, T>::MINB)) yrow_kernel(YRArgs a)
 {
     using G = YRGeom<L, T>;
     using C = typename G::C;
@@ -465,14 +467,14 @@ static int launch_yrow_l(Ctx *c, const YRArgs &a, double bytes)
     }
     const unsigned grid = (unsigned)((c->nx + G::ROWS - 1) / G::ROWS);
     prof_begin(c, KC_FUSED_Y, bytes);
-    yrow_kernel<L, T><<<grid, G::T_ * G::ROWS, smem, c->stream>>>(a);
+    yrow_kernel<L, T><<<grid, G::THREADS, smem, c->stream>>>(a);
     prof_end(c);
     MHD_CHECK_LAUNCH();
     return MHDGPU_OK;
 }
 
-// Whether the row kernel serves this context (16 <= ny <= 4096).
-bool yrow_supported(const Ctx *c) { return c->ny >= 16 && c->ny <= 4096; }
+// Whether the row kernel serves this context (16 <= ny <= 8192).
+bool yrow_supported(const Ctx *c) { return c->ny >= 16 && c->ny <= 8192; }
 
 int launch_yrow(Ctx *c, int iRK, int last_stage, int mode)
 {
@@ -538,6 +540,7 @@ int launch_yrow(Ctx *c, int iRK, int last_stage, int mode)
         case 1024: return launch_yrow_l<10, float>(c, a, b);
         case 2048: return launch_yrow_l<11, float>(c, a, b);
         case 4096: return launch_yrow_l<12, float>(c, a, b);
+        case 8192: return launch_yrow_l<13, float>(c, a, b);
         default: return mhd_set_error(MHDGPU_ERR_UNSUPPORTED);
         }
     }
@@ -551,6 +554,7 @@ int launch_yrow(Ctx *c, int iRK, int last_stage, int mode)
     case 1024: return launch_yrow_l<10, double>(c, a, bytes);
     case 2048: return launch_yrow_l<11, double>(c, a, bytes);
     case 4096: return launch_yrow_l<12, double>(c, a, bytes);
+    case 8192: return launch_yrow_l<13, double>(c, a, bytes);
     default: return mhd_set_error(MHDGPU_ERR_UNSUPPORTED);
     }
 }
