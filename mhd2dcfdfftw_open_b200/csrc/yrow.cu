@@ -70,8 +70,12 @@ struct YRGeom {
     // shared memory: one padded FFT row per row of the CTA (68 KB in FP64,
     // 34 KB in FP32, for rows up to 4096 points; twice that for 8192)
     static constexpr size_t SMEM = sizeof(C) * ROWS * NP;
-    // CTAs per SM the register budget is set for
-    static constexpr int MINB = THREADS > YR_THREADS ? 1 : (sizeof(T) == 8 ? 2 : 3);
+    // CTAs per SM the register budget is set for.  Measured at 4096^2 on one
+    // B200: FP64 at 2 (128 registers) 5.05 ms per launch, at 3 (80) 5.88 ms;
+    // FP32 at 2 5.04 ms, 3 4.11 ms, 4 (64 registers, 136 KB of shared memory
+    // per SM) 3.65 ms -- more resident rows beat fewer spills, up to where
+    // the spills reach the FP64 working set
+    static constexpr int MINB = THREADS > YR_THREADS ? 1 : (sizeof(T) == 8 ? 2 : 4);
 };
 
 // Load fields fa and fb (fb < 0: zero) of this group's row into the FFT row
