@@ -496,10 +496,18 @@ __device__ __forceinline__ void xn_chunk(const XNCommon &k, const XNTaps<NT> &tp
 }
 
 
+// CTAs per SM the register budget is set for.  Measured at 4096^2 on one
+// B200 (per launch, FP64 / FP32 derivatives / FP64 filter): 1 CTA bound
+// (254 registers, no spills) 1.58 / - / 1.60 ms; 3 (168) 1.28 / 1.22 /
+// 1.51 ms; 4 (128) 1.40 / 1.18 / 1.60 ms.  The spills this costs stay in L1;
+// the extra resident warps hide the latency of the inflow loads.
+template <typename T>
+constexpr int xn_minb() { return sizeof(T) == 8 ? 3 : 4; }
+
 // One warp per chunk, NW chunks (consecutive along the line) per CTA, 32
 // columns per CTA; blockIdx.z: the job.
 template <int L, typename T, int UNR, int NW>
-__global__ void __launch_bounds__(32 * NW) xd_kernel(const __grid_constant__ XDParams P)
+__global__ void __launch_bounds__(32 * NW, xn_minb<T>()) xd_kernel(const __grid_constant__ XDParams P)
 {
     const int lane = threadIdx.x & 31;
     const long j = (long)blockIdx.x * 32 + lane;
@@ -537,7 +545,7 @@ __global__ void __launch_bounds__(32 * NW) xd_kernel(const __grid_constant__ XDP
 }
 
 template <int L, typename T, int UNR, int NW>
-__global__ void __launch_bounds__(32 * NW) xf_kernel(const __grid_constant__ XFParams P)
+__global__ void __launch_bounds__(32 * NW, xn_minb<T>()) xf_kernel(const __grid_constant__ XFParams P)
 {
     static_assert(sizeof(T) == 8, "the x filter runs in FP64 in both precisions");
     const int lane = threadIdx.x & 31;
