@@ -113,6 +113,17 @@ int mhdgpu_stage(mhdgpu_ctx *ctx, int iRK);
 int mhdgpu_steps(mhdgpu_ctx *ctx, int nsteps, double dt_fixed, double *dt_io);
 /* Same steps through the fused two-pass stage (x pass + y pass per stage). */
 int mhdgpu_steps_fused(mhdgpu_ctx *ctx, int nsteps, double dt_fixed, double *dt_io);
+/* A stream of independent states (no counterpart in the reference): for r <
+ * nstates, the state (NVAR*nx*ny doubles, the uu layout) at h_in[r] is
+ * advanced by nsteps fused steps, each from *dt_io as mhdgpu_steps_fused
+ * would after mhdgpu_set_array(UU), and written to h_out[r] (no h_out[r] may
+ * overlap an h_in[k], k > r; the same pointer may repeat within h_in and
+ * within h_out).  Uploads and downloads run on
+ * their own streams while the previous/next state steps; page-locked host
+ * buffers let them overlap.  *dt_io returns the last state's dt.  Afterwards
+ * the context holds the last state, as after mhdgpu_steps_fused. */
+int mhdgpu_steps_fused_stream(mhdgpu_ctx *ctx, int nstates, const double *const *h_in,
+                              double *const *h_out, int nsteps, double dt_fixed, double *dt_io);
 
 /* Arithmetic of mhdgpu_steps_fused (no counterpart in the reference, which
  * computes in FP64 only).  MHDGPU_PRECISION_FP64 (the default) follows the

@@ -133,6 +133,15 @@ static void destroy_locked(mhdgpu_ctx *h)
         free(c->prof_ev);
         free(c->prof_cls);
     }
+    cudaFree(c->xfer_in);
+    cudaFree(c->xfer_out);
+    for (int i = 0; i < 2; i++)
+        if (c->xfer_s[i]) {
+            cudaStreamSynchronize(c->xfer_s[i]);
+            cudaStreamDestroy(c->xfer_s[i]);
+        }
+    for (int i = 0; i < 4; i++)
+        if (c->xfer_ev[i]) cudaEventDestroy(c->xfer_ev[i]);
     if (c->stream) cudaStreamDestroy(c->stream);
     delete c;
 }
@@ -604,6 +613,73 @@ extern "C" int mhdgpu_autotune(mhdgpu_ctx *h, int *columns_out)
             }
     MHD_CUDA_TRY(cudaStreamSynchronize(c->stream));
     return check_flag(c);
+}
+
+// A stream of independent states through the fused steps (no counterpart
+// in the reference, whose driver advances one state): state r is uploaded
+// from h_in[r], advanced by nsteps steps exactly as mhdgpu_steps_fused
+// advances a state set with mhdgpu_set_array, and downloaded to h_out[r].
+// The upload of state r+1 (into a device staging copy, on its own stream)
+// and the download of state r-1 (from a second staging copy, on a third
+// stream) run while state r steps; with page-locked host buffers the
+// transfers and the steps overlap.
+extern "C" int mhdgpu_steps_fused_stream(mhdgpu_ctx *h, int nstates, const double *const *h_in,
+                                         double *const *h_out, int nsteps, double dt_fixed,
+                                         double *dt_io)
+{
+    CTX_OR_FAIL(h);
+    if (nstates < 0 || nsteps < 0 || (nstates > 0 && (!h_in || !h_out)))
+        return mhd_set_error(MHDGPU_ERR_INVALID);
+    for (int r = 0; r < nstates; r++)
+        if (!h_in[r] || !h_out[r]) return mhd_set_error(MHDGPU_ERR_INVALID);
+    if (nstates == 0) return MHDGPU_OK;
+    const size_t bytes = sizeof(double) * c->nvar * c->nx * c->ny;
+    if (!c->xfer_in) {
+        MHD_CUDA_TRY(cudaMalloc(&c->xfer_in, bytes));
+        MHD_CUDA_TRY(cudaMalloc(&c->xfer_out, bytes));
+        for (int i = 0; i < 2; i++)
+            MHD_CUDA_TRY(cudaStreamCreateWithFlags(&c->xfer_s[i], cudaStreamNonBlocking));
+        for (int i = 0; i < 4; i++)
+            MHD_CUDA_TRY(cudaEventCreateWithFlags(&c->xfer_ev[i], cudaEventDisableTiming));
+    }
+    cudaStream_t sin = c->xfer_s[0], sout = c->xfer_s[1];
+    cudaEvent_t in_ready = c->xfer_ev[0], in_free = c->xfer_ev[1];
+    cudaEvent_t out_ready = c->xfer_ev[2], out_free = c->xfer_ev[3];
+    double *uu = c->arr[MHDGPU_UU];
+    const double dt0 = dt_io ? *dt_io : 0.0;
+    double dt = dt0;
+    int rc = MHDGPU_OK;
+    MHD_CUDA_TRY(cudaMemcpyAsync(c->xfer_in, h_in[0], bytes, cudaMemcpyHostToDevice, sin));
+    MHD_CUDA_TRY(cudaEventRecord(in_ready, sin));
+    for (int r = 0; r < nstates && rc == MHDGPU_OK; r++) {
+        MHD_CUDA_TRY(cudaStreamWaitEvent(c->stream, in_ready, 0));
+        MHD_CUDA_TRY(cudaMemcpyAsync(uu, c->xfer_in, bytes, cudaMemcpyDeviceToDevice, c->stream));
+        MHD_CUDA_TRY(cudaEventRecord(in_free, c->stream));
+        c->fused_pending_filter = 0;  // as mhdgpu_set_array(UU)
+        c->state_in_S = 0;
+        if (r + 1 < nstates) {
+            MHD_CUDA_TRY(cudaStreamWaitEvent(sin, in_free, 0));
+            MHD_CUDA_TRY(cudaMemcpyAsync(c->xfer_in, h_in[r + 1], bytes, cudaMemcpyHostToDevice, sin));
+            MHD_CUDA_TRY(cudaEventRecord(in_ready, sin));
+        }
+        double d = dt0;
+        rc = mhdgpu_steps_fused(h, nsteps, dt_fixed, &d);
+        if (rc != MHDGPU_OK) break;
+        dt = d;
+        // the previous state's download has left the outgoing copy
+        if (r > 0) MHD_CUDA_TRY(cudaStreamWaitEvent(c->stream, out_free, 0));
+        MHD_CUDA_TRY(cudaMemcpyAsync(c->xfer_out, uu, bytes, cudaMemcpyDeviceToDevice, c->stream));
+        MHD_CUDA_TRY(cudaEventRecord(out_ready, c->stream));
+        MHD_CUDA_TRY(cudaStreamWaitEvent(sout, out_ready, 0));
+        MHD_CUDA_TRY(cudaMemcpyAsync(h_out[r], c->xfer_out, bytes, cudaMemcpyDeviceToHost, sout));
+        MHD_CUDA_TRY(cudaEventRecord(out_free, sout));
+    }
+    // no copy of this call is left in flight, also after an error
+    const cudaError_t e0 = cudaStreamSynchronize(sin), e1 = cudaStreamSynchronize(sout);
+    if (rc != MHDGPU_OK) return rc;
+    if (e0 != cudaSuccess || e1 != cudaSuccess) return mhd_set_error(MHDGPU_ERR_CUDA);
+    if (dt_io) *dt_io = dt;
+    return MHDGPU_OK;
 }
 
 extern "C" int mhdgpu_set_precision(mhdgpu_ctx *h, int precision)

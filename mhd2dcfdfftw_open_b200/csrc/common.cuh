@@ -109,6 +109,12 @@ struct Ctx {
     int xn_on;                   // the fused steps use it
     double *xn_state;            // nvar planes
     int state_in_S;              // the current, x-filtered state is in xn_state
+    // streaming of independent states (mhdgpu_steps_fused_stream): device
+    // staging copies of an incoming and an outgoing state, the copy streams
+    // and their events (in ready, in free, out ready, out free)
+    double *xfer_in, *xfer_out;
+    cudaStream_t xfer_s[2];
+    cudaEvent_t xfer_ev[4];
 };
 
 }  // namespace mhd

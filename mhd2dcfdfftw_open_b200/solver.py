@@ -42,6 +42,7 @@ EXPORTED = (
     "mhdgpu_calc_efield", "mhdgpu_calc_divb", "mhdgpu_calc_rhs", "mhdgpu_rk_init",
     "mhdgpu_rk_execute", "mhdgpu_filtering", "mhdgpu_calc_dt", "mhdgpu_check_divb",
     "mhdgpu_get_cleaning_speeds", "mhdgpu_stage", "mhdgpu_steps", "mhdgpu_steps_fused",
+    "mhdgpu_steps_fused_stream",
     "mhdgpu_diagnostics", "mhdgpu_state_cells", "mhdgpu_stream", "mhdgpu_launch_count", "mhdgpu_profile",
     "mhdgpu_profile_read", "mhdgpu_set_precision", "mhdgpu_autotune", "mhdgpu_selftest_wait",
 )
@@ -94,6 +95,8 @@ def load_library(path: str = LIB_PATH):
     L.mhdgpu_stage.argtypes = [vp, ctypes.c_int]
     L.mhdgpu_steps.argtypes = [vp, ctypes.c_int, ctypes.c_double, dp]
     L.mhdgpu_steps_fused.argtypes = [vp, ctypes.c_int, ctypes.c_double, dp]
+    L.mhdgpu_steps_fused_stream.argtypes = [vp, ctypes.c_int, ctypes.POINTER(dp), ctypes.POINTER(dp),
+                                            ctypes.c_int, ctypes.c_double, dp]
     L.mhdgpu_set_precision.argtypes = [vp, ctypes.c_int]
     L.mhdgpu_autotune.argtypes = [vp, ctypes.POINTER(ctypes.c_int)]
     L.mhdgpu_selftest_wait.argtypes = [vp, ctypes.c_double]
@@ -231,6 +234,27 @@ class Domain:
         d = ctypes.c_double(dt)
         f = self.lib.mhdgpu_steps_fused if fused else self.lib.mhdgpu_steps
         self._check(f(self.h, int(nsteps), float(dt_fixed), ctypes.byref(d)))
+        return d.value
+
+    def steps_stream(self, inputs, outputs, nsteps, dt_fixed, dt=0.0):
+        """Advance each state of `inputs` (arrays shaped like uu) by nsteps
+        fused steps from dt, independently, into the matching array of
+        `outputs` (C-contiguous float64, preferably page-locked); transfers
+        overlap the steps of the neighbouring states.  Returns the last
+        state's dt (mhdgpu_steps_fused_stream)."""
+        if len(inputs) != len(outputs):
+            raise ValueError("inputs and outputs differ in length")
+        shape = (self.nvar, self.p.nx, self.p.ny)
+        for a in list(inputs) + list(outputs):
+            if a.shape != shape or a.dtype != np.float64 or not a.flags.c_contiguous:
+                raise ValueError("states must be C-contiguous float64 arrays of shape %s" % (shape,))
+        n = len(inputs)
+        dp = ctypes.POINTER(ctypes.c_double)
+        pin = (dp * n)(*[_dptr(a) for a in inputs])
+        pout = (dp * n)(*[_dptr(a) for a in outputs])
+        d = ctypes.c_double(dt)
+        self._check(self.lib.mhdgpu_steps_fused_stream(self.h, n, pin, pout, int(nsteps),
+                                                       float(dt_fixed), ctypes.byref(d)))
         return d.value
 
     def set_precision(self, mixed):
