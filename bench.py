@@ -466,7 +466,7 @@ def main():
     ap.add_argument("--path", choices=["fused", "operators"], default="fused")
     ap.add_argument("--nx", type=int, default=4096)
     ap.add_argument("--ny", type=int, default=4096)
-    ap.add_argument("--e2e-steps", type=int, default=10)
+    ap.add_argument("--e2e-steps", type=int, default=20)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--precision", choices=["fp64", "mixed"], default="fp64")
     ap.add_argument("--workload", choices=["turbulence", "parametric"], default="turbulence")
