@@ -497,12 +497,14 @@ __device__ __forceinline__ void xn_chunk(const XNCommon &k, const XNTaps<NT> &tp
 
 
 // CTAs per SM the register budget is set for.  Measured at 4096^2 on one
-// B200 (per launch, FP64 / FP32 derivatives / FP64 filter): 1 CTA bound
-// (254 registers, no spills) 1.58 / - / 1.60 ms; 3 (168) 1.28 / 1.22 /
-// 1.51 ms; 4 (128) 1.40 / 1.18 / 1.60 ms.  The spills this costs stay in L1;
-// the extra resident warps hide the latency of the inflow loads.
+// B200 (per launch, FP64 / FP32 derivatives / FP64 filter), with 4 chunks
+// per CTA: 1 CTA bound (254 registers, no spills) 1.58 / - / 1.60 ms; 3 (168)
+// 1.28 / 1.22 / 1.51 ms; 4 (128) 1.40 / 1.18 / 1.60 ms.  With 2 chunks per
+// CTA at the same registers (6 and 8 CTAs): 1.23 / 1.16 / 1.46 ms.  The
+// spills this costs stay in L1; the extra resident warps hide the latency of
+// the inflow loads.
 template <typename T>
-constexpr int xn_minb() { return sizeof(T) == 8 ? 3 : 4; }
+constexpr int xn_minb() { return sizeof(T) == 8 ? 6 : 8; }
 
 // One warp per chunk, NW chunks (consecutive along the line) per CTA, 32
 // columns per CTA; blockIdx.z: the job.
@@ -567,9 +569,10 @@ __global__ void __launch_bounds__(32 * NW, xn_minb<T>()) xf_kernel(const __grid_
 // ---------------------------------------------------------------------------
 // host side: set-up and launches
 // ---------------------------------------------------------------------------
-// chunks (one warp each) per CTA: 4 measured faster than 8 on B200 (fewer
-// registers' worth of CTAs to place, the same L1 reuse of the inflow rows)
-constexpr int XN_NW = 4;
+// chunks (one warp each) per CTA: at one CTA per SM 4 measured faster than
+// 8, and at the register budget of xn_minb 2 faster than 4 (smaller CTAs to
+// place; the L1 reuse of the inflow rows is per SM either way)
+constexpr int XN_NW = 2;
 constexpr int XN_LD = 16;  // rows per chunk of the derivative kernel
 constexpr int XN_LF = 32;  // rows per chunk of the filter kernel
 // Lines shorter than this keep the cluster x pass (xline.cu), which holds a
