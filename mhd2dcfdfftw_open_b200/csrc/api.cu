@@ -648,32 +648,38 @@ extern "C" int mhdgpu_steps_fused_stream(mhdgpu_ctx *h, int nstates, const doubl
     double *uu = c->arr[MHDGPU_UU];
     const double dt0 = dt_io ? *dt_io : 0.0;
     double dt = dt0;
-    int rc = MHDGPU_OK;
-    MHD_CUDA_TRY(cudaMemcpyAsync(c->xfer_in, h_in[0], bytes, cudaMemcpyHostToDevice, sin));
-    MHD_CUDA_TRY(cudaEventRecord(in_ready, sin));
-    for (int r = 0; r < nstates && rc == MHDGPU_OK; r++) {
-        MHD_CUDA_TRY(cudaStreamWaitEvent(c->stream, in_ready, 0));
-        MHD_CUDA_TRY(cudaMemcpyAsync(uu, c->xfer_in, bytes, cudaMemcpyDeviceToDevice, c->stream));
-        MHD_CUDA_TRY(cudaEventRecord(in_free, c->stream));
-        c->fused_pending_filter = 0;  // as mhdgpu_set_array(UU)
-        c->state_in_S = 0;
-        if (r + 1 < nstates) {
-            MHD_CUDA_TRY(cudaStreamWaitEvent(sin, in_free, 0));
-            MHD_CUDA_TRY(cudaMemcpyAsync(c->xfer_in, h_in[r + 1], bytes, cudaMemcpyHostToDevice, sin));
-            MHD_CUDA_TRY(cudaEventRecord(in_ready, sin));
+    // the copies and steps; every error path leaves through the
+    // synchronisation below, so no copy of the caller's buffers is in flight
+    // when the call returns
+    auto run = [&]() -> int {
+        MHD_CUDA_TRY(cudaMemcpyAsync(c->xfer_in, h_in[0], bytes, cudaMemcpyHostToDevice, sin));
+        MHD_CUDA_TRY(cudaEventRecord(in_ready, sin));
+        for (int r = 0; r < nstates; r++) {
+            MHD_CUDA_TRY(cudaStreamWaitEvent(c->stream, in_ready, 0));
+            MHD_CUDA_TRY(cudaMemcpyAsync(uu, c->xfer_in, bytes, cudaMemcpyDeviceToDevice, c->stream));
+            MHD_CUDA_TRY(cudaEventRecord(in_free, c->stream));
+            c->fused_pending_filter = 0;  // as mhdgpu_set_array(UU)
+            c->state_in_S = 0;
+            if (r + 1 < nstates) {
+                MHD_CUDA_TRY(cudaStreamWaitEvent(sin, in_free, 0));
+                MHD_CUDA_TRY(cudaMemcpyAsync(c->xfer_in, h_in[r + 1], bytes, cudaMemcpyHostToDevice, sin));
+                MHD_CUDA_TRY(cudaEventRecord(in_ready, sin));
+            }
+            double d = dt0;
+            const int rs = mhdgpu_steps_fused(h, nsteps, dt_fixed, &d);
+            if (rs != MHDGPU_OK) return rs;
+            dt = d;
+            // the previous state's download has left the outgoing copy
+            if (r > 0) MHD_CUDA_TRY(cudaStreamWaitEvent(c->stream, out_free, 0));
+            MHD_CUDA_TRY(cudaMemcpyAsync(c->xfer_out, uu, bytes, cudaMemcpyDeviceToDevice, c->stream));
+            MHD_CUDA_TRY(cudaEventRecord(out_ready, c->stream));
+            MHD_CUDA_TRY(cudaStreamWaitEvent(sout, out_ready, 0));
+            MHD_CUDA_TRY(cudaMemcpyAsync(h_out[r], c->xfer_out, bytes, cudaMemcpyDeviceToHost, sout));
+            MHD_CUDA_TRY(cudaEventRecord(out_free, sout));
         }
-        double d = dt0;
-        rc = mhdgpu_steps_fused(h, nsteps, dt_fixed, &d);
-        if (rc != MHDGPU_OK) break;
-        dt = d;
-        // the previous state's download has left the outgoing copy
-        if (r > 0) MHD_CUDA_TRY(cudaStreamWaitEvent(c->stream, out_free, 0));
-        MHD_CUDA_TRY(cudaMemcpyAsync(c->xfer_out, uu, bytes, cudaMemcpyDeviceToDevice, c->stream));
-        MHD_CUDA_TRY(cudaEventRecord(out_ready, c->stream));
-        MHD_CUDA_TRY(cudaStreamWaitEvent(sout, out_ready, 0));
-        MHD_CUDA_TRY(cudaMemcpyAsync(h_out[r], c->xfer_out, bytes, cudaMemcpyDeviceToHost, sout));
-        MHD_CUDA_TRY(cudaEventRecord(out_free, sout));
-    }
+        return MHDGPU_OK;
+    };
+    const int rc = run();
     // no copy of this call is left in flight, also after an error
     const cudaError_t e0 = cudaStreamSynchronize(sin), e1 = cudaStreamSynchronize(sout);
     if (rc != MHDGPU_OK) return rc;
